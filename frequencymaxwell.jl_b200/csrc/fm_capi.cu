@@ -1,0 +1,1262 @@
+// libfmcuda: plan object, CBS operator drivers, Krylov drivers and the C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fmcuda.h"
+#include "fm_krylov.cuh"
+#include "fm_launch.h"
+#include "fm_setup.cuh"
+
+using namespace fm;
+using cd = std::complex<double>;
+
+static thread_local std::string g_err;
+
+static fm_status fail(fm_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define FM_CK(expr)                                                                              \
+  do {                                                                                           \
+    cudaError_t e_ = (expr);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      return fail(e_ == cudaErrorMemoryAllocation ? FM_ERR_OOM : FM_ERR_CUDA,                    \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                          \
+    }                                                                                            \
+  } while (0)
+
+#define FM_TRY(expr)               \
+  do {                             \
+    fm_status s_ = (expr);         \
+    if (s_ != FM_OK) return s_;    \
+  } while (0)
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+bool is_pow2_in(int n, int lo, int hi) { return n >= lo && n <= hi && (n & (n - 1)) == 0; }
+
+}  // namespace
+
+struct fm_plan {
+  fm_plan_desc desc{};
+  int prec = FM_PREC_F32;
+  size_t esz = 8;  // bytes per complex element
+  Dims dims{};
+  PadInfo pi{};
+  long long n = 0, M = 0;  // voxels, elements per field (3n)
+  cudaStream_t st = nullptr;
+  bool avg = false;     // any absorbing axis
+  bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
+  double shift[3] = {0, 0, 0};
+  // potential / physics
+  bool have_pot = false;
+  double k_bg = 0, eps_imag = 0, wavelength = 0, kref2 = 1;
+  int bornmax = 0;
+  // tables (plan precision)
+  DevBuf twx, twy, twz, twz2, rz, rxp, rxm, ryp, rym, rzp, rzm;
+  DevBuf V;
+  // workspace
+  DevBuf t1, t2, bbuf, xbuf, ebuf, sbuf, basis, gbuf2;
+  DevBuf red_part, red_out, red_cnt, active, scale, coef, hbuf;
+  DevBuf eps_dev, fx, fy, fz, maxpart, maxout;
+  DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
+  DevBuf Eo, Ho;
+  int out_nrhs = 0;
+};
+
+// ---------------------------------------------------------------------------
+// tables
+// ---------------------------------------------------------------------------
+template <typename R>
+static cudaError_t upload_cplx(DevBuf& buf, const std::vector<cd>& v, cudaStream_t st) {
+  using T = cplx<R>;
+  std::vector<T> h(v.size());
+  for (size_t i = 0; i < v.size(); ++i) h[i] = mk((R)v[i].real(), (R)v[i].imag());
+  cudaError_t e = buf.ensure(std::max<size_t>(1, h.size()) * sizeof(T));
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(buf.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(st);
+}
+
+static std::vector<cd> twiddles(int L) {
+  std::vector<cd> t(L);
+  for (int k = 0; k < L; ++k) {
+    double a = -2.0 * M_PI * (double)k / (double)L;
+    t[k] = cd(std::cos(a), std::sin(a));
+  }
+  return t;
+}
+
+// exp(sgn * 2 pi i * idx * s / L)
+static std::vector<cd> ramp(int L, double s, double sgn) {
+  std::vector<cd> t(L);
+  for (int k = 0; k < L; ++k) {
+    double a = sgn * 2.0 * M_PI * (double)k * s / (double)L;
+    t[k] = cd(std::cos(a), std::sin(a));
+  }
+  return t;
+}
+
+template <typename R>
+static fm_status init_tables(fm_plan* P) {
+  FM_CK(upload_cplx<R>(P->twx, twiddles(P->dims.nx), P->st));
+  FM_CK(upload_cplx<R>(P->twy, twiddles(P->dims.ny), P->st));
+  FM_CK(upload_cplx<R>(P->twz, twiddles(P->dims.nz), P->st));
+  if (P->zonly) {
+    FM_CK(upload_cplx<R>(P->twz2, twiddles(2 * P->dims.nz), P->st));
+    FM_CK(upload_cplx<R>(P->rz, ramp(P->dims.nz, P->shift[2], -1.0), P->st));
+  } else if (P->avg) {
+    FM_CK(upload_cplx<R>(P->rxp, ramp(P->dims.nx, P->shift[0], -1.0), P->st));
+    FM_CK(upload_cplx<R>(P->rxm, ramp(P->dims.nx, P->shift[0], +1.0), P->st));
+    FM_CK(upload_cplx<R>(P->ryp, ramp(P->dims.ny, P->shift[1], -1.0), P->st));
+    FM_CK(upload_cplx<R>(P->rym, ramp(P->dims.ny, P->shift[1], +1.0), P->st));
+    FM_CK(upload_cplx<R>(P->rzp, ramp(P->dims.nz, P->shift[2], -1.0), P->st));
+    FM_CK(upload_cplx<R>(P->rzm, ramp(P->dims.nz, P->shift[2], +1.0), P->st));
+  }
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// workspace
+// ---------------------------------------------------------------------------
+static int red_blocks(const fm_plan* P, int nb) {
+  int sms = 148;
+  int per = std::max(1, (4 * sms + nb - 1) / nb);
+  long long chunk = (long long)KV_THREADS * KV_EPT;
+  long long maxb = (P->M + chunk - 1) / chunk;
+  return (int)std::max(1LL, std::min<long long>(per, maxb));
+}
+
+static fm_status ensure_reduce(fm_plan* P, int nb, int K) {
+  const int nblk = red_blocks(P, nb);
+  FM_CK(P->red_part.ensure((size_t)nb * nblk * (KV_KMAX + 2) * sizeof(double2)));
+  FM_CK(P->red_out.ensure((size_t)nb * (KV_KMAX + 2) * sizeof(double2)));
+  if (P->red_cnt.cap < (size_t)nb * sizeof(unsigned)) {
+    FM_CK(P->red_cnt.ensure((size_t)nb * sizeof(unsigned)));
+    FM_CK(cudaMemsetAsync(P->red_cnt.p, 0, (size_t)nb * sizeof(unsigned), P->st));
+  }
+  (void)K;
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Green application / CBS operator on device buffers (plan precision)
+//   in  : nb fields
+//   out : nb fields (may not alias in, t1, t2)
+//   pro : PRO_COPY (psi = in) or PRO_V / PRO_V_SCALE (psi = V.*in [* scale])
+//   epi : EPI_* epilogue applied to g = G_avg(psi)
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
+                          const void* bv, const EpiParams& ep, void* out, const int* act) {
+  using T = cplx<R>;
+  Dims d = P->dims;
+  d.nb = nb;
+  const size_t fbytes = (size_t)nb * P->M * sizeof(T);
+  FM_CK(P->t1.ensure(fbytes));
+  FM_CK(P->t2.ensure(fbytes));
+  GreenParams gp{};
+  const double kr = std::sqrt(P->kref2);
+  for (int a = 0; a < 3; ++a) gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]) / kr;
+  gp.ksq_re = P->k_bg * P->k_bg / P->kref2;
+  gp.ksq_im = P->eps_imag / P->kref2;
+  const void* V = P->V.p;
+  if (!P->avg || P->zonly) {
+    const int mode = P->zonly ? ZMODE_AVG2 : ZMODE_ONE;
+    gp.shift[2] = P->zonly ? P->shift[2] : 0.0;
+    gp.scale_re = 1.0 / ((double)P->n * (P->zonly ? 2.0 : 1.0));
+    FM_CK(launch_xf<R>(d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act, P->st));
+    FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act, P->st));
+    FM_CK(launch_zg<R>(d, mode, P->t2.p, gp, P->zonly ? P->twz2.p : P->twz.p, P->zonly ? P->rz.p : nullptr, P->t1.p,
+                       act, P->st));
+    FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act, P->st));
+    FM_CK(launch_xi<R>(d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act, P->st));
+    return FM_OK;
+  }
+  // general case (sub-pixel shifts on x or y): the two branches run separately and are averaged
+  return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build (only z)");
+}
+
+// ---------------------------------------------------------------------------
+// Krylov helpers
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status multidot(fm_plan* P, int nb, int K, const void* U, const void* w, bool wnorm, const int* act,
+                          std::vector<double2>& host_out) {
+  FM_TRY(ensure_reduce(P, nb, K));
+  const int nblk = red_blocks(P, nb);
+  dim3 g(nblk, nb);
+  if (wnorm)
+    k_multidot<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
+                                                     (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                     (unsigned*)P->red_cnt.p, act);
+  else
+    k_multidot<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
+                                                      (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                      (unsigned*)P->red_cnt.p, act);
+  FM_CK(cudaGetLastError());
+  const int KK = K + (wnorm ? 1 : 0);
+  host_out.resize((size_t)nb * KK);
+  FM_CK(cudaMemcpyAsync(host_out.data(), P->red_out.p, host_out.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  return FM_OK;
+}
+
+// y = ca*a + cb*b + cc*c per RHS (host coefficient vectors of length nb, empty -> operand skipped)
+template <typename R>
+static fm_status axpby3(fm_plan* P, int nb, const void* a, const std::vector<cd>& ca, const void* b,
+                        const std::vector<cd>& cb, const void* c, const std::vector<cd>& cc, void* y, bool norm,
+                        const int* act, std::vector<double>* nrm) {
+  FM_TRY(ensure_reduce(P, nb, 1));
+  FM_CK(P->coef.ensure((size_t)3 * nb * sizeof(double2)));
+  std::vector<double2> h((size_t)3 * nb, make_double2(0, 0));
+  for (int i = 0; i < nb; ++i) {
+    if (a) h[i] = make_double2(ca[i].real(), ca[i].imag());
+    if (b) h[nb + i] = make_double2(cb[i].real(), cb[i].imag());
+    if (c) h[2 * nb + i] = make_double2(cc[i].real(), cc[i].imag());
+  }
+  FM_CK(cudaMemcpyAsync(P->coef.p, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  const double2* cp = (const double2*)P->coef.p;
+  const int nblk = red_blocks(P, nb);
+  dim3 g(nblk, nb);
+  using T = cplx<R>;
+  if (norm)
+    k_axpby3<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c, cp + 2 * nb,
+                                                   (T*)y, (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                   (unsigned*)P->red_cnt.p, act);
+  else
+    k_axpby3<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c,
+                                                    cp + 2 * nb, (T*)y, nullptr, nullptr, nullptr, act);
+  FM_CK(cudaGetLastError());
+  if (norm) {
+    std::vector<double2> o(nb);
+    FM_CK(cudaMemcpyAsync(o.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+    nrm->resize(nb);
+    for (int i = 0; i < nb; ++i) (*nrm)[i] = o[i].x;
+  }
+  return FM_OK;
+}
+
+static void sym_givens(cd a, double b, double& c, cd& s, cd& rho) {
+  const double aa = std::abs(a);
+  if (b == 0.0) {
+    c = 1.0;
+    s = 0.0;
+    rho = a;
+  } else if (aa == 0.0) {
+    c = 0.0;
+    s = 1.0;
+    rho = b;
+  } else {
+    const double r = std::hypot(aa, b);
+    c = aa / r;
+    s = (a / aa) * (b / r);
+    rho = (a / aa) * r;
+  }
+}
+
+struct RhsState {
+  bool active = true;
+  bool solved = false;
+  int iters = 0;
+  double beta = 0, eps = 0, rnorm = 0;
+  std::vector<double> c;
+  std::vector<cd> s, z;
+  std::vector<std::vector<cd>> R;  // columns
+  int inner = 0;
+};
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// ---------------------------------------------------------------------------
+// GMRES (Krylov.jl semantics) on a batch of nb RHS; b in P->bbuf, x (warm
+// start u0 = b) in P->xbuf.  Basis vectors are kept unnormalised with their
+// scale 1/h_{k+1,k} in P->scale (deferred normalisation).
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info, double deadline) {
+  using T = cplx<R>;
+  const size_t fe = (size_t)P->M;
+  const size_t fbytes = (size_t)nb * fe * sizeof(T);
+  const int itmax = std::max(1, o.maxiters);
+  const int mem = (o.restart > 0) ? std::min(o.restart, itmax) : itmax;
+  if (mem + 1 > KV_KMAX) return fail(FM_ERR_UNSUPPORTED, "Krylov basis larger than 127 vectors");
+  FM_CK(P->basis.ensure((size_t)(mem + 1) * fbytes));
+  FM_CK(P->scale.ensure((size_t)(KV_KMAX + 1) * nb * sizeof(double)));
+  FM_CK(P->hbuf.ensure((size_t)nb * (KV_KMAX + 2) * sizeof(double2)));
+  FM_CK(P->active.ensure((size_t)nb * sizeof(int)));
+  FM_TRY(ensure_reduce(P, nb, mem + 1));
+  T* U = (T*)P->basis.p;
+  double* sc = (double*)P->scale.p;
+  int* act = (int*)P->active.p;
+  const double btol = std::pow(2.220446049250313e-16, 0.75);
+
+  std::vector<RhsState> S(nb);
+  std::vector<int> acth(nb, 1);
+  std::vector<double> sch((size_t)(KV_KMAX + 1) * nb, 0.0);
+  EpiParams ep{};
+  ep.inv_eps = P->kref2 / P->eps_imag;
+  auto upload_active = [&]() -> fm_status {
+    FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+    return FM_OK;
+  };
+  auto upload_scale_col = [&](int j) -> fm_status {
+    FM_CK(cudaMemcpyAsync(sc + (size_t)j * nb, sch.data() + (size_t)j * nb, nb * sizeof(double), cudaMemcpyHostToDevice,
+                          P->st));
+    return FM_OK;
+  };
+  // r0 = M^{-1}(b - A x) into U[0]
+  auto residual_into_U0 = [&](const int* a) -> fm_status {
+    return green_op<R>(P, nb, P->xbuf.p, PRO_V, nullptr, EPI_PREC_RES, P->xbuf.p, P->bbuf.p, ep, U, a);
+  };
+
+  FM_TRY(upload_active());
+  FM_TRY(residual_into_U0(act));
+  std::vector<double2> hv;
+  FM_TRY(multidot<R>(P, nb, 0, U, U, true, act, hv));
+  int iter = 0;
+  for (int b = 0; b < nb; ++b) {
+    S[b].beta = std::sqrt(hv[b].x);
+    S[b].rnorm = S[b].beta;
+    S[b].eps = o.abstol + o.reltol * S[b].beta;
+    info[b].residual0 = S[b].beta;
+    if (S[b].beta == 0.0) {
+      S[b].active = false;
+      S[b].solved = true;
+      acth[b] = 0;
+    } else if (S[b].rnorm <= S[b].eps) {
+      S[b].active = false;
+      S[b].solved = true;
+      acth[b] = 0;
+    }
+  }
+  bool any = false;
+  for (int b = 0; b < nb; ++b) any |= S[b].active;
+  std::vector<int> started(nb, 0);
+  while (any && iter < itmax) {
+    // (re)start: U[0] = r0 (already for the first pass), z[0] = beta
+    for (int b = 0; b < nb; ++b) {
+      if (!S[b].active) continue;
+      S[b].c.clear(); S[b].s.clear(); S[b].R.clear(); S[b].z.assign(1, cd(S[b].beta, 0)); S[b].inner = 0;
+      sch[b] = 1.0 / S[b].beta;
+    }
+    FM_TRY(upload_active());
+    FM_TRY(upload_scale_col(0));
+    int j = 0;
+    bool pass_done = false;
+    while (!pass_done) {
+      // w = M^{-1} A v_j  into U[j+1]
+      T* Uj = U + (size_t)j * nb * fe;
+      T* Uw = U + (size_t)(j + 1) * nb * fe;
+      FM_TRY(green_op<R>(P, nb, Uj, PRO_V_SCALE, sc + (size_t)j * nb, EPI_PREC_OP, Uj, nullptr, ep, Uw, act));
+      // orthogonalise against v_0..v_j
+      const int K = j + 1;
+      std::vector<double2> hcol((size_t)nb * (K + 1));
+      const int nblk = red_blocks(P, nb);
+      dim3 g(nblk, nb);
+      if (o.ortho == FM_ORTHO_MGS) {
+        double2* hd = (double2*)P->hbuf.p;
+        const int hs = KV_KMAX + 2;
+        for (int i = 0; i <= K; ++i) {
+          k_mgs<R><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, i, K, U, sc, nb, Uw, hd, hs, (double2*)P->red_part.p,
+                                                (unsigned*)P->red_cnt.p, act);
+        }
+        FM_CK(cudaGetLastError());
+        std::vector<double2> hh((size_t)nb * hs);
+        FM_CK(cudaMemcpyAsync(hh.data(), hd, hh.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+        FM_CK(cudaStreamSynchronize(P->st));
+        for (int b = 0; b < nb; ++b)
+          for (int i = 0; i <= K; ++i) hcol[(size_t)b * (K + 1) + i] = hh[(size_t)b * hs + i];
+      } else {
+        // classical Gram-Schmidt (optionally twice), FP64 coefficients
+        std::vector<double2> hr;
+        FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr));
+        std::vector<double2> htot((size_t)nb * K);
+        for (int b = 0; b < nb; ++b)
+          for (int i = 0; i < K; ++i) {
+            double s = sch[(size_t)i * nb + b];
+            htot[(size_t)b * K + i] = make_double2(hr[(size_t)b * K + i].x * s, hr[(size_t)b * K + i].y * s);
+          }
+        const int passes = (o.ortho == FM_ORTHO_CGS2) ? 2 : 1;
+        for (int pass = 0; pass < passes; ++pass) {
+          const bool last = (pass == passes - 1);
+          // raw projections <U_i, w>; the update coefficient of U_i is sc_i^2 * hr_i
+          FM_CK(P->coef.ensure((size_t)nb * K * sizeof(double2)));
+          FM_CK(cudaMemcpyAsync(P->coef.p, hr.data(), hr.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+          Coef cf{(const double2*)P->coef.p, K, sc, nb, -1.0, 0};
+          if (last)
+            k_update<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr, (double2*)P->red_part.p,
+                                                           (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act);
+          else
+            k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr, nullptr, nullptr, nullptr,
+                                                            act);
+          FM_CK(cudaGetLastError());
+          if (!last) {
+            FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr));
+            for (int b = 0; b < nb; ++b)
+              for (int i = 0; i < K; ++i) {
+                double s = sch[(size_t)i * nb + b];
+                htot[(size_t)b * K + i].x += hr[(size_t)b * K + i].x * s;
+                htot[(size_t)b * K + i].y += hr[(size_t)b * K + i].y * s;
+              }
+          }
+        }
+        std::vector<double2> nn(nb);
+        FM_CK(cudaMemcpyAsync(nn.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+        FM_CK(cudaStreamSynchronize(P->st));
+        for (int b = 0; b < nb; ++b) {
+          for (int i = 0; i < K; ++i) hcol[(size_t)b * (K + 1) + i] = htot[(size_t)b * K + i];
+          hcol[(size_t)b * (K + 1) + K] = nn[b];
+        }
+      }
+      ++iter;
+      // Givens update per RHS
+      bool any_left = false;
+      for (int b = 0; b < nb; ++b) {
+        RhsState& r = S[b];
+        if (!r.active) continue;
+        std::vector<cd> col(K);
+        for (int i = 0; i < K; ++i) col[i] = cd(hcol[(size_t)b * (K + 1) + i].x, hcol[(size_t)b * (K + 1) + i].y);
+        const double hb = std::sqrt(std::max(0.0, hcol[(size_t)b * (K + 1) + K].x));
+        for (int i = 0; i < K - 1; ++i) {
+          cd t = r.c[i] * col[i] + r.s[i] * col[i + 1];
+          col[i + 1] = std::conj(r.s[i]) * col[i] - r.c[i] * col[i + 1];
+          col[i] = t;
+        }
+        double c;
+        cd s, rho;
+        sym_givens(col[K - 1], hb, c, s, rho);
+        col[K - 1] = rho;
+        r.c.push_back(c);
+        r.s.push_back(s);
+        r.R.push_back(col);
+        const cd zk1 = std::conj(s) * r.z[K - 1];
+        r.z[K - 1] = c * r.z[K - 1];
+        r.rnorm = std::abs(zk1);
+        r.inner = K;
+        r.iters += 1;
+        const bool solved = (r.rnorm <= r.eps) || (r.rnorm + 1.0 <= 1.0);
+        const bool breakdown = hb <= btol;
+        const bool tired = iter >= itmax;
+        const bool inner_tired = K >= mem;
+        r.solved = solved;
+        if (solved || breakdown || tired || inner_tired) {
+          acth[b] = 0;  // this pass is over for b
+          if (solved || breakdown || tired) r.active = false;
+        } else {
+          r.z.push_back(zk1);
+          sch[(size_t)(j + 1) * nb + b] = 1.0 / hb;
+          any_left = true;
+        }
+        if (breakdown) r.active = false;
+      }
+      if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
+      if (!any_left) {
+        pass_done = true;
+      } else {
+        FM_TRY(upload_active());
+        FM_TRY(upload_scale_col(j + 1));
+        ++j;
+      }
+    }
+    // x += sum_i y_i v_i  per RHS that took part in this pass
+    std::vector<double2> yh((size_t)nb * (KV_KMAX + 1), make_double2(0, 0));
+    int Kmax = 0;
+    for (int b = 0; b < nb; ++b) {
+      RhsState& r = S[b];
+      const int n_in = r.inner;
+      if (n_in == 0) continue;
+      std::vector<cd> y(r.z.begin(), r.z.begin() + n_in);
+      for (int i = n_in - 1; i >= 0; --i) {
+        for (int jj = n_in - 1; jj > i; --jj) y[i] -= r.R[jj][i] * y[jj];
+        if (std::abs(r.R[i][i]) <= btol) {
+          for (int q = 0; q <= i; ++q) y[q] = 0.0;
+          break;
+        }
+        y[i] /= r.R[i][i];
+      }
+      for (int i = 0; i < n_in; ++i) yh[(size_t)b * (KV_KMAX + 1) + i] = make_double2(y[i].real(), y[i].imag());
+      Kmax = std::max(Kmax, n_in);
+      r.inner = 0;
+    }
+    if (Kmax > 0) {
+      FM_CK(P->coef.ensure(yh.size() * sizeof(double2)));
+      FM_CK(cudaMemcpyAsync(P->coef.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+      FM_CK(cudaMemcpyAsync(sc, sch.data(), (size_t)(KV_KMAX + 1) * nb * sizeof(double), cudaMemcpyHostToDevice, P->st));
+      Coef cf{(const double2*)P->coef.p, KV_KMAX + 1, sc, nb, 1.0, 1};
+      dim3 g(red_blocks(P, nb), nb);
+      k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, Kmax, U, cf, (T*)P->xbuf.p, nullptr, nullptr, nullptr,
+                                                      nullptr, nullptr);
+      FM_CK(cudaGetLastError());
+    }
+    any = false;
+    for (int b = 0; b < nb; ++b) {
+      acth[b] = S[b].active ? 1 : 0;
+      any |= S[b].active;
+    }
+    if (any && iter < itmax) {
+      // restart: new residual for the RHS still running
+      FM_TRY(upload_active());
+      FM_TRY(residual_into_U0(act));
+      FM_TRY(multidot<R>(P, nb, 0, U, U, true, act, hv));
+      for (int b = 0; b < nb; ++b)
+        if (S[b].active) S[b].beta = std::sqrt(hv[b].x);
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    info[b].iterations = S[b].iters;
+    info[b].solved = S[b].solved ? 1 : 0;
+    info[b].residual = S[b].rnorm;
+  }
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab (left preconditioned, Krylov.jl form, shadow c = b) and the plain
+// Born series (Richardson) on the same operator.
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status bicgstab(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info, double deadline) {
+  using T = cplx<R>;
+  const size_t fe = (size_t)P->M, fbytes = (size_t)nb * fe * sizeof(T);
+  // r, p, v, s, t, dx in the basis buffer
+  FM_CK(P->basis.ensure(6 * fbytes));
+  FM_CK(P->active.ensure((size_t)nb * sizeof(int)));
+  T* base = (T*)P->basis.p;
+  T *r = base, *p = base + nb * fe, *v = base + 2 * nb * fe, *s = base + 3 * nb * fe, *t = base + 4 * nb * fe,
+    *dx = base + 5 * nb * fe;
+  int* act = (int*)P->active.p;
+  std::vector<int> acth(nb, 1);
+  EpiParams ep{};
+  ep.inv_eps = P->kref2 / P->eps_imag;
+  FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  FM_TRY(green_op<R>(P, nb, P->xbuf.p, PRO_V, nullptr, EPI_PREC_RES, P->xbuf.p, P->bbuf.p, ep, r, act));
+  FM_CK(cudaMemcpyAsync(p, r, fbytes, cudaMemcpyDeviceToDevice, P->st));
+  FM_CK(cudaMemsetAsync(dx, 0, fbytes, P->st));
+  std::vector<double2> hv;
+  FM_TRY(multidot<R>(P, nb, 1, P->bbuf.p, r, true, act, hv));  // <c, r>, ||r||^2
+  std::vector<cd> rho(nb), next_rho(nb), alpha(nb), omega(nb);
+  std::vector<double> rn(nb), eps(nb);
+  std::vector<int> iters(nb, 0);
+  std::vector<bool> solved(nb, false), active(nb, true);
+  for (int b = 0; b < nb; ++b) {
+    rn[b] = std::sqrt(hv[2 * b + 1].x);
+    info[b].residual0 = rn[b];
+    eps[b] = o.abstol + o.reltol * rn[b];
+    next_rho[b] = cd(hv[2 * b].x, hv[2 * b].y);
+    if (rn[b] == 0.0 || rn[b] <= eps[b]) { solved[b] = true; active[b] = false; }
+    else if (next_rho[b] == 0.0) { active[b] = false; }
+  }
+  auto sync_active = [&]() -> fm_status {
+    bool any = false;
+    for (int b = 0; b < nb; ++b) { acth[b] = active[b] ? 1 : 0; any |= active[b]; }
+    FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+    return any ? FM_OK : FM_NOT_CONVERGED;  // NOT_CONVERGED used as "nothing left" sentinel
+  };
+  int iter = 0;
+  std::vector<cd> one(nb, 1.0), z(nb);
+  while (iter < o.maxiters) {
+    if (sync_active() != FM_OK) break;
+    ++iter;
+    for (int b = 0; b < nb; ++b) rho[b] = next_rho[b];
+    FM_TRY(green_op<R>(P, nb, p, PRO_V, nullptr, EPI_PREC_OP, p, nullptr, ep, v, act));
+    FM_TRY(multidot<R>(P, nb, 1, P->bbuf.p, v, false, act, hv));
+    std::vector<cd> ma(nb), a(nb);
+    for (int b = 0; b < nb; ++b) {
+      if (!active[b]) continue;
+      alpha[b] = rho[b] / cd(hv[b].x, hv[b].y);
+      ma[b] = -alpha[b];
+      a[b] = alpha[b];
+    }
+    FM_TRY(axpby3<R>(P, nb, r, one, v, ma, nullptr, z, s, false, act, nullptr));   // s = r - alpha v
+    FM_TRY(axpby3<R>(P, nb, dx, one, p, a, nullptr, z, dx, false, act, nullptr));  // dx += alpha p
+    FM_TRY(green_op<R>(P, nb, s, PRO_V, nullptr, EPI_PREC_OP, s, nullptr, ep, t, act));
+    std::vector<double2> ts, tt;
+    FM_TRY(multidot<R>(P, nb, 1, t, s, false, act, ts));
+    FM_TRY(multidot<R>(P, nb, 1, t, t, false, act, tt));
+    std::vector<cd> om(nb), mom(nb), beta(nb);
+    for (int b = 0; b < nb; ++b) {
+      if (!active[b]) continue;
+      omega[b] = cd(ts[b].x, ts[b].y) / cd(tt[b].x, tt[b].y);
+      om[b] = omega[b];
+      mom[b] = -omega[b];
+    }
+    FM_TRY(axpby3<R>(P, nb, dx, one, s, om, nullptr, z, dx, false, act, nullptr));  // dx += omega s
+    std::vector<double> nr;
+    FM_TRY(axpby3<R>(P, nb, s, one, t, mom, nullptr, z, r, true, act, &nr));        // r = s - omega t
+    FM_TRY(multidot<R>(P, nb, 1, P->bbuf.p, r, false, act, hv));
+    for (int b = 0; b < nb; ++b) {
+      if (!active[b]) continue;
+      next_rho[b] = cd(hv[b].x, hv[b].y);
+      beta[b] = (next_rho[b] / rho[b]) * (alpha[b] / omega[b]);
+    }
+    // p = r + beta (p - omega v)
+    std::vector<cd> bm(nb), bw(nb);
+    for (int b = 0; b < nb; ++b) { bm[b] = beta[b]; bw[b] = -beta[b] * omega[b]; }
+    FM_TRY(axpby3<R>(P, nb, r, one, p, bm, v, bw, p, false, act, nullptr));
+    for (int b = 0; b < nb; ++b) {
+      if (!active[b]) continue;
+      rn[b] = std::sqrt(nr[b]);
+      iters[b] = iter;
+      const bool ok = rn[b] <= eps[b] || (rn[b] + 1.0 <= 1.0);
+      solved[b] = ok;
+      if (ok || alpha[b] == 0.0 || std::isnan(alpha[b].real())) active[b] = false;
+    }
+    if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
+  }
+  // x = x0 + dx
+  std::vector<cd> onev(nb, 1.0);
+  FM_TRY(axpby3<R>(P, nb, P->xbuf.p, onev, dx, onev, nullptr, z, P->xbuf.p, false, nullptr, nullptr));
+  for (int b = 0; b < nb; ++b) {
+    info[b].iterations = iters[b];
+    info[b].solved = solved[b] ? 1 : 0;
+    info[b].residual = rn[b];
+  }
+  return FM_OK;
+}
+
+template <typename R>
+static fm_status richardson(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info,
+                            double deadline) {
+  using T = cplx<R>;
+  const size_t fe = (size_t)P->M, fbytes = (size_t)nb * fe * sizeof(T);
+  FM_CK(P->basis.ensure(fbytes));
+  FM_CK(P->active.ensure((size_t)nb * sizeof(int)));
+  T* r = (T*)P->basis.p;
+  int* act = (int*)P->active.p;
+  std::vector<int> acth(nb, 1);
+  EpiParams ep{};
+  ep.inv_eps = P->kref2 / P->eps_imag;
+  std::vector<double> rn(nb), eps(nb);
+  std::vector<int> iters(nb, 0);
+  std::vector<bool> solved(nb, false), active(nb, true);
+  std::vector<cd> one(nb, 1.0), z(nb);
+  std::vector<double2> hv;
+  int iter = 0;
+  while (true) {
+    bool any = false;
+    for (int b = 0; b < nb; ++b) { acth[b] = active[b] ? 1 : 0; any |= active[b]; }
+    if (!any) break;
+    FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+    FM_TRY(green_op<R>(P, nb, P->xbuf.p, PRO_V, nullptr, EPI_PREC_RES, P->xbuf.p, P->bbuf.p, ep, r, act));
+    FM_TRY(multidot<R>(P, nb, 0, r, r, true, act, hv));
+    for (int b = 0; b < nb; ++b) {
+      if (!active[b]) continue;
+      rn[b] = std::sqrt(hv[b].x);
+      if (iter == 0) { eps[b] = o.abstol + o.reltol * rn[b]; info[b].residual0 = rn[b]; }
+      iters[b] = iter;
+      if (rn[b] <= eps[b]) { solved[b] = true; active[b] = false; }
+      else if (iter >= o.maxiters) active[b] = false;
+      acth[b] = active[b] ? 1 : 0;
+    }
+    FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+    FM_TRY(axpby3<R>(P, nb, P->xbuf.p, one, r, one, nullptr, z, P->xbuf.p, false, act, nullptr));
+    ++iter;
+    if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
+  }
+  for (int b = 0; b < nb; ++b) {
+    info[b].iterations = iters[b];
+    info[b].solved = solved[b] ? 1 : 0;
+    info[b].residual = rn[b];
+  }
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// shared solve core: from scaled source terms in P->sbuf (nb RHS) to the
+// scattered field in P->xbuf and its curl in P->ebuf.
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info) {
+  using T = cplx<R>;
+  const size_t fbytes = (size_t)nb * P->M * sizeof(T);
+  const double deadline = o.timeout_s > 0 ? now_s() + o.timeout_s : 0.0;
+  FM_CK(P->bbuf.ensure(fbytes));
+  FM_CK(P->xbuf.ensure(fbytes));
+  FM_CK(P->ebuf.ensure(fbytes));
+  EpiParams ep{};
+  // b = G_avg S ; x0 = b
+  FM_TRY(green_op<R>(P, nb, P->sbuf.p, PRO_COPY, nullptr, EPI_STORE, nullptr, nullptr, ep, P->bbuf.p, nullptr));
+  FM_CK(cudaMemcpyAsync(P->xbuf.p, P->bbuf.p, fbytes, cudaMemcpyDeviceToDevice, P->st));
+  fm_status st;
+  if (o.method == FM_METHOD_GMRES) st = gmres<R>(P, nb, o, info, deadline);
+  else if (o.method == FM_METHOD_BICGSTAB) st = bicgstab<R>(P, nb, o, info, deadline);
+  else if (o.method == FM_METHOD_RICHARDSON) st = richardson<R>(P, nb, o, info, deadline);
+  else return fail(FM_ERR_INVALID, "unknown method");
+  if (st != FM_OK) return st;
+  // H_s = -i lambda/(2 pi 377) curl(E_s)
+  Dims d = P->dims;
+  d.nb = nb;
+  FM_CK(P->t1.ensure(fbytes));
+  FM_CK(P->t2.ensure(fbytes));
+  GreenParams gp{};
+  for (int a = 0; a < 3; ++a)
+    gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]);
+  const double f = P->wavelength / (2.0 * M_PI * 377.0) / (double)P->n;
+  gp.scale_re = 0.0;
+  gp.scale_im = -f;
+  FM_CK(launch_xf<R>(d, PRO_COPY, P->xbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr, P->st));
+  FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
+  FM_CK(launch_zg<R>(d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr, P->st));
+  FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
+  FM_CK(launch_xi<R>(d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
+                     nullptr, P->st));
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host <-> device conversions
+// ---------------------------------------------------------------------------
+template <typename R>
+static fm_status h2d_field(fm_plan* P, const double* host, long long count, double s, void* dst) {
+  FM_CK(P->gbuf2.ensure((size_t)count * sizeof(double2)));
+  FM_CK(cudaMemcpyAsync(P->gbuf2.p, host, (size_t)count * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  k_from_f64<R><<<1184, 256, 0, P->st>>>(count, (const double2*)P->gbuf2.p, s, (cplx<R>*)dst);
+  FM_CK(cudaGetLastError());
+  return FM_OK;
+}
+template <typename R>
+static fm_status d2h_field(fm_plan* P, const void* src, long long count, double s, double* host) {
+  FM_CK(P->gbuf2.ensure((size_t)count * sizeof(double2)));
+  k_to_f64<R><<<1184, 256, 0, P->st>>>(count, (const cplx<R>*)src, s, (double2*)P->gbuf2.p);
+  FM_CK(cudaGetLastError());
+  FM_CK(cudaMemcpyAsync(host, P->gbuf2.p, (size_t)count * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  return FM_OK;
+}
+
+static fm_status check_plan(fm_plan* P, int nrhs, bool need_pot) {
+  if (!P) return fail(FM_ERR_INVALID, "null plan");
+  if (nrhs < 1) return fail(FM_ERR_INVALID, "nrhs must be >= 1");
+  if (need_pot && !P->have_pot) return fail(FM_ERR_INVALID, "potential not set (fm_set_potential / fm_build_potential)");
+  FM_CK(cudaSetDevice(P->desc.device));
+  return FM_OK;
+}
+
+static fm_status validate_opts(const fm_solve_opts* o) {
+  if (!o) return fail(FM_ERR_INVALID, "null options");
+  if (o->maxiters < 1) return fail(FM_ERR_INVALID, "maxiters must be >= 1");
+  if (!(o->reltol >= 0 && o->reltol <= 1)) return fail(FM_ERR_INVALID, "tolerance must be in [0, 1]");
+  if (!(o->abstol >= 0)) return fail(FM_ERR_INVALID, "abstol must be >= 0");
+  if (o->method < 0 || o->method > 2) return fail(FM_ERR_INVALID, "unknown method");
+  if (o->ortho < 0 || o->ortho > 2) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
+  if (o->restart < 0) return fail(FM_ERR_INVALID, "restart must be >= 0");
+  if (o->method == FM_METHOD_GMRES) {
+    const int mem = o->restart > 0 ? std::min(o->restart, o->maxiters) : o->maxiters;
+    if (mem + 1 > KV_KMAX) return fail(FM_ERR_UNSUPPORTED, "GMRES basis larger than 127 vectors (use restart)");
+  }
+  return FM_OK;
+}
+
+template <typename R>
+static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, int& wave) {
+  size_t freeb = 0, totalb = 0;
+  FM_CK(cudaMemGetInfo(&freeb, &totalb));
+  const size_t fb = (size_t)P->M * sizeof(cplx<R>);
+  int vecs = 0;
+  if (o.method == FM_METHOD_GMRES) vecs = (o.restart > 0 ? std::min(o.restart, o.maxiters) : o.maxiters) + 1;
+  else if (o.method == FM_METHOD_BICGSTAB) vecs = 6;
+  else vecs = 1;
+  // basis + b + x + s + e + t1 + t2 + fp64 staging and outputs
+  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 3;
+  const size_t held = P->basis.cap + P->bbuf.cap + P->xbuf.cap + P->sbuf.cap + P->ebuf.cap + P->t1.cap + P->t2.cap +
+                      P->gbuf2.cap + P->Eo.cap + P->Ho.cap;
+  const size_t avail = (size_t)((freeb + held) * 0.92);
+  wave = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, avail / per));
+  wave = std::min(wave, std::max(1, P->desc.max_rhs));
+  if ((size_t)wave * per > avail) return fail(FM_ERR_OOM, "one right-hand side does not fit in device memory");
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI (C linkage comes from the declarations in fmcuda.h)
+// ---------------------------------------------------------------------------
+
+int fm_abi_version(void) { return FMCUDA_ABI_VERSION; }
+const char* fm_last_error(void) { return g_err.c_str(); }
+int fm_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+long long fm_plan_bytes(const fm_plan_desc* d, int nrhs, int basis) {
+  if (!d) return -1;
+  long long n = 1;
+  for (int a = 0; a < 3; ++a) n *= (long long)(d->grid[a] + 2 * d->pad[a]);
+  const long long fb = 3 * n * (d->precision == FM_PREC_F64 ? 16 : 8);
+  return fb * (long long)nrhs * (basis + 6) + n * (d->precision == FM_PREC_F64 ? 16 : 8) +
+         3LL * n * 16 * nrhs;
+}
+
+fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
+  if (!desc || !out) return fail(FM_ERR_INVALID, "null argument");
+  *out = nullptr;
+  for (int a = 0; a < 3; ++a) {
+    if (desc->grid[a] <= 0) return fail(FM_ERR_INVALID, "all grid_size components must be positive");
+    if (desc->pad[a] < 0) return fail(FM_ERR_INVALID, "padding must be >= 0");
+    if (!(desc->resolution[a] > 0)) return fail(FM_ERR_INVALID, "all resolution components must be positive");
+  }
+  if (desc->precision != FM_PREC_F32 && desc->precision != FM_PREC_F64)
+    return fail(FM_ERR_INVALID, "precision must be FM_PREC_F32 or FM_PREC_F64");
+  int nd = 0;
+  if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) return fail(FM_ERR_CUDA, "no CUDA device");
+  if (desc->device < 0 || desc->device >= nd) return fail(FM_ERR_INVALID, "device ordinal out of range");
+  const int n3[3] = {desc->grid[0] + 2 * desc->pad[0], desc->grid[1] + 2 * desc->pad[1], desc->grid[2] + 2 * desc->pad[2]};
+  for (int a = 0; a < 3; ++a)
+    if (!is_pow2_in(n3[a], 8, AXIS_MAX))
+      return fail(FM_ERR_UNSUPPORTED, "padded axis sizes must be powers of two in [8, 512] in this build");
+  bool avg = desc->absorbing[0] || desc->absorbing[1] || desc->absorbing[2];
+  bool zonly = desc->absorbing[2] && !desc->absorbing[0] && !desc->absorbing[1];
+  if (avg && !zonly) return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build");
+  if (zonly && n3[2] > AXIS_MAX_AVG2)
+    return fail(FM_ERR_UNSUPPORTED, "padded z size above 256 with an absorbing z boundary is not supported by this build");
+  const int prec = desc->precision;
+  const int pwy = prec == FM_PREC_F64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
+  const int pwz = prec == FM_PREC_F64 ? pencils_per_warp<double>(zonly ? 2 * n3[2] : n3[2])
+                                      : pencils_per_warp<float>(zonly ? 2 * n3[2] : n3[2]);
+  if (pwy <= 0 || pwz <= 0 || n3[0] % pwy || n3[0] % pwz) return fail(FM_ERR_UNSUPPORTED, "x size too small for pencil tiling");
+  if (cudaSetDevice(desc->device) != cudaSuccess) return fail(FM_ERR_CUDA, "cudaSetDevice failed");
+  fm_plan* P = new fm_plan();
+  P->desc = *desc;
+  if (P->desc.max_rhs < 1) P->desc.max_rhs = 1;
+  P->prec = prec;
+  P->esz = prec == FM_PREC_F64 ? 16 : 8;
+  P->dims = Dims{n3[0], n3[1], n3[2], 1, (long long)n3[0] * n3[1] * n3[2]};
+  P->n = P->dims.n;
+  P->M = 3 * P->n;
+  P->pi = PadInfo{desc->grid[0], desc->grid[1], desc->grid[2], desc->pad[0], desc->pad[1], desc->pad[2], n3[0], n3[1], n3[2]};
+  P->avg = avg;
+  P->zonly = zonly;
+  for (int a = 0; a < 3; ++a) P->shift[a] = desc->absorbing[a] ? 0.25 : 0.0;
+  if (cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete P;
+    return fail(FM_ERR_CUDA, "stream creation failed");
+  }
+  fm_status s = prec == FM_PREC_F64 ? init_tables<double>(P) : init_tables<float>(P);
+  if (s != FM_OK) {
+    fm_plan_destroy(P);
+    return s;
+  }
+  *out = P;
+  return FM_OK;
+}
+
+void fm_plan_destroy(fm_plan* P) {
+  if (!P) return;
+  cudaSetDevice(P->desc.device);
+  if (P->st) cudaStreamSynchronize(P->st);
+  DevBuf* bufs[] = {&P->twx, &P->twy, &P->twz, &P->twz2, &P->rz, &P->rxp, &P->rxm, &P->ryp, &P->rym, &P->rzp,
+                    &P->rzm, &P->V, &P->t1, &P->t2, &P->bbuf, &P->xbuf, &P->ebuf, &P->sbuf, &P->basis,
+                    &P->gbuf2, &P->red_part, &P->red_out, &P->red_cnt, &P->active, &P->scale, &P->coef,
+                    &P->hbuf, &P->eps_dev, &P->fx, &P->fy, &P->fz, &P->maxpart, &P->maxout, &P->wt_x,
+                    &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho};
+  for (DevBuf* b : bufs) b->release();
+  if (P->st) cudaStreamDestroy(P->st);
+  delete P;
+}
+
+fm_status fm_synchronize(fm_plan* P) {
+  if (!P) return fail(FM_ERR_INVALID, "null plan");
+  FM_CK(cudaSetDevice(P->desc.device));
+  FM_CK(cudaStreamSynchronize(P->st));
+  return FM_OK;
+}
+
+static void set_scalars(fm_plan* P, double k_bg, double eps_imag, double wavelength) {
+  P->k_bg = k_bg;
+  P->eps_imag = eps_imag;
+  P->wavelength = wavelength;
+  P->kref2 = (k_bg > 0) ? k_bg * k_bg : 1.0;
+}
+
+fm_status fm_set_potential(fm_plan* P, const double* V, double k_bg, double eps_imag, double wavelength) {
+  FM_TRY(check_plan(P, 1, false));
+  if (!V) return fail(FM_ERR_INVALID, "null potential");
+  if (!(k_bg > 0) || !(eps_imag > 0) || !(wavelength > 0)) return fail(FM_ERR_INVALID, "k_bg, eps_imag, wavelength must be positive");
+  set_scalars(P, k_bg, eps_imag, wavelength);
+  FM_CK(P->V.ensure((size_t)P->n * P->esz));
+  if (P->prec == FM_PREC_F64) FM_TRY(h2d_field<double>(P, V, P->n, 1.0 / P->kref2, P->V.p));
+  else FM_TRY(h2d_field<float>(P, V, P->n, 1.0 / P->kref2, P->V.p));
+  FM_CK(cudaStreamSynchronize(P->st));
+  P->have_pot = true;
+  return FM_OK;
+}
+
+template <typename R>
+static fm_status apply_host(fm_plan* P, int nrhs, const double* x, double* y, int mode, cd alpha, cd beta) {
+  const long long cnt = (long long)nrhs * P->M;
+  const size_t fbytes = (size_t)cnt * sizeof(cplx<R>);
+  FM_CK(P->sbuf.ensure(fbytes));
+  FM_CK(P->ebuf.ensure(fbytes));
+  EpiParams ep{};
+  ep.alpha_re = alpha.real();
+  ep.alpha_im = alpha.imag();
+  ep.beta_re = beta.real();
+  ep.beta_im = beta.imag();
+  ep.inv_eps = P->kref2 / P->eps_imag;
+  if (mode == 0) {  // Green: input scaled by 1/kref2 so that G' x' = G x
+    FM_TRY(h2d_field<R>(P, x, cnt, 1.0 / P->kref2, P->sbuf.p));
+    FM_TRY(green_op<R>(P, nrhs, P->sbuf.p, PRO_COPY, nullptr, EPI_STORE, nullptr, nullptr, ep, P->ebuf.p, nullptr));
+  } else if (mode == 1) {  // operator
+    FM_TRY(h2d_field<R>(P, x, cnt, 1.0, P->sbuf.p));
+    if (beta != 0.0) FM_TRY(h2d_field<R>(P, y, cnt, 1.0, P->ebuf.p));
+    FM_TRY(green_op<R>(P, nrhs, P->sbuf.p, PRO_V, nullptr, EPI_OP, P->sbuf.p, nullptr, ep, P->ebuf.p, nullptr));
+  } else if (mode == 2) {  // curl
+    FM_TRY(h2d_field<R>(P, x, cnt, 1.0, P->sbuf.p));
+    Dims d = P->dims;
+    d.nb = nrhs;
+    FM_CK(P->t1.ensure(fbytes));
+    FM_CK(P->t2.ensure(fbytes));
+    GreenParams gp{};
+    for (int a = 0; a < 3; ++a)
+      gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]);
+    gp.scale_im = -P->wavelength / (2.0 * M_PI * 377.0) / (double)P->n;
+    FM_CK(launch_xf<R>(d, PRO_COPY, P->sbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr, P->st));
+    FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
+    FM_CK(launch_zg<R>(d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr, P->st));
+    FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
+    FM_CK(launch_xi<R>(d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
+                       nullptr, P->st));
+  }
+  FM_TRY(d2h_field<R>(P, P->ebuf.p, cnt, 1.0, y));
+  return FM_OK;
+}
+
+fm_status fm_green_apply(fm_plan* P, int nrhs, const double* x, double* y) {
+  FM_TRY(check_plan(P, nrhs, true));
+  if (!x || !y) return fail(FM_ERR_INVALID, "null buffer");
+  return P->prec == FM_PREC_F64 ? apply_host<double>(P, nrhs, x, y, 0, 0.0, 0.0) : apply_host<float>(P, nrhs, x, y, 0, 0.0, 0.0);
+}
+
+fm_status fm_apply_operator(fm_plan* P, int nrhs, const double* x, double* y, double ar, double ai, double br, double bi) {
+  FM_TRY(check_plan(P, nrhs, true));
+  if (!x || !y) return fail(FM_ERR_INVALID, "null buffer");
+  return P->prec == FM_PREC_F64 ? apply_host<double>(P, nrhs, x, y, 1, cd(ar, ai), cd(br, bi))
+                                : apply_host<float>(P, nrhs, x, y, 1, cd(ar, ai), cd(br, bi));
+}
+
+fm_status fm_curl_field(fm_plan* P, int nrhs, const double* E, double* H) {
+  FM_TRY(check_plan(P, nrhs, false));
+  if (!E || !H) return fail(FM_ERR_INVALID, "null buffer");
+  if (!(P->wavelength > 0)) return fail(FM_ERR_INVALID, "wavelength not set (fm_set_potential / fm_build_potential)");
+  return P->prec == FM_PREC_F64 ? apply_host<double>(P, nrhs, E, H, 2, 0.0, 0.0) : apply_host<float>(P, nrhs, E, H, 2, 0.0, 0.0);
+}
+
+template <typename R>
+__global__ void k_precond(long long n, int nb, const cplx<R>* __restrict__ V, double inv_eps, const cplx<R>* __restrict__ x,
+                          cplx<R>* __restrict__ y) {
+  const long long tot = n * 3 * nb;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+    cplx<R> v = V[i % n];
+    cplx<R> g = mk(-v.y * (R)inv_eps, v.x * (R)inv_eps);
+    y[i] = cmul(g, x[i]);
+  }
+}
+
+template <typename R>
+static fm_status precond_host(fm_plan* P, int nrhs, const double* x, double* y) {
+  const long long cnt = (long long)nrhs * P->M;
+  FM_CK(P->sbuf.ensure((size_t)cnt * sizeof(cplx<R>)));
+  FM_CK(P->ebuf.ensure((size_t)cnt * sizeof(cplx<R>)));
+  FM_TRY(h2d_field<R>(P, x, cnt, 1.0, P->sbuf.p));
+  k_precond<R><<<1184, 256, 0, P->st>>>(P->n, nrhs, (const cplx<R>*)P->V.p, P->kref2 / P->eps_imag,
+                                        (const cplx<R>*)P->sbuf.p, (cplx<R>*)P->ebuf.p);
+  FM_CK(cudaGetLastError());
+  return d2h_field<R>(P, P->ebuf.p, cnt, 1.0, y);
+}
+
+fm_status fm_apply_preconditioner(fm_plan* P, int nrhs, const double* x, double* y) {
+  FM_TRY(check_plan(P, nrhs, true));
+  if (!x || !y) return fail(FM_ERR_INVALID, "null buffer");
+  return P->prec == FM_PREC_F64 ? precond_host<double>(P, nrhs, x, y) : precond_host<float>(P, nrhs, x, y);
+}
+
+template <typename R>
+static fm_status solve_source_t(fm_plan* P, int nrhs, const double* S, const fm_solve_opts& o, double* E, double* H,
+                                fm_solve_info* info) {
+  int wave = 1;
+  FM_TRY(plan_wave_size<R>(P, nrhs, o, wave));
+  bool all_ok = true;
+  for (int b0 = 0; b0 < nrhs; b0 += wave) {
+    const int nb = std::min(wave, nrhs - b0);
+    const long long cnt = (long long)nb * P->M;
+    FM_CK(P->sbuf.ensure((size_t)cnt * sizeof(cplx<R>)));
+    FM_TRY(h2d_field<R>(P, S + (size_t)b0 * P->M * 2, cnt, 1.0 / P->kref2, P->sbuf.p));
+    std::vector<fm_solve_info> inf(nb);
+    FM_TRY(solve_core<R>(P, nb, o, inf));
+    FM_TRY(d2h_field<R>(P, P->xbuf.p, cnt, 1.0, E + (size_t)b0 * P->M * 2));
+    FM_TRY(d2h_field<R>(P, P->ebuf.p, cnt, 1.0, H + (size_t)b0 * P->M * 2));
+    for (int b = 0; b < nb; ++b) {
+      if (info) info[b0 + b] = inf[b];
+      all_ok &= inf[b].solved != 0;
+    }
+  }
+  if (!all_ok) return fail(FM_NOT_CONVERGED, "iteration limit reached before the tolerance was met");
+  return FM_OK;
+}
+
+fm_status fm_solve_source(fm_plan* P, int nrhs, const double* S, const fm_solve_opts* opts, double* E, double* H,
+                          fm_solve_info* info) {
+  FM_TRY(check_plan(P, nrhs, true));
+  FM_TRY(validate_opts(opts));
+  if (!S || !E || !H) return fail(FM_ERR_INVALID, "null buffer");
+  return P->prec == FM_PREC_F64 ? solve_source_t<double>(P, nrhs, S, *opts, E, H, info)
+                                : solve_source_t<float>(P, nrhs, S, *opts, E, H, info);
+}
+
+template <typename R>
+static fm_status build_potential_t(fm_plan* P, const double* eps, double eps_bg, double wl, const double* fx,
+                                   const double* fy, const double* fz, int itmax, fm_potential_info* info) {
+  const long long g = (long long)P->pi.gx * P->pi.gy * P->pi.gz;
+  FM_CK(P->eps_dev.ensure((size_t)g * sizeof(double2)));
+  FM_CK(cudaMemcpyAsync(P->eps_dev.p, eps, (size_t)g * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  {
+    // NaN/Inf in the permittivity would propagate silently (fmax ignores NaN): reject it here
+    FM_CK(P->maxout.ensure(sizeof(double) + sizeof(unsigned) + sizeof(unsigned long long) + 8));
+    unsigned long long* bad = (unsigned long long*)((char*)P->maxout.p + 16);
+    FM_CK(cudaMemsetAsync(bad, 0, sizeof(unsigned long long), P->st));
+    k_count_nonfinite<double><<<592, 256, 0, P->st>>>(g, (const double2*)P->eps_dev.p, bad);
+    FM_CK(cudaGetLastError());
+    unsigned long long nbad = 0;
+    FM_CK(cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+    if (nbad) return fail(FM_ERR_NONFINITE, "permittivity contains NaN or Inf");
+  }
+  const int nb = 592;
+  FM_CK(P->maxpart.ensure(nb * sizeof(double)));
+  unsigned* cnt = (unsigned*)((char*)P->maxout.p + sizeof(double));
+  FM_CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned), P->st));
+  const double k_bg = 2.0 * M_PI * std::sqrt(eps_bg) / wl;
+  const double k2 = k_bg * k_bg;
+  k_potential_max<<<nb, 256, 0, P->st>>>(g, (const double2*)P->eps_dev.p, eps_bg, k2, (double*)P->maxpart.p,
+                                          (double*)P->maxout.p, cnt);
+  FM_CK(cudaGetLastError());
+  double vmax = 0.0;
+  FM_CK(cudaMemcpyAsync(&vmax, P->maxout.p, sizeof(double), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  if (!std::isfinite(vmax)) return fail(FM_ERR_NONFINITE, "non-finite permittivity");
+  // with padding the zero-padded region also enters the maximum (|0| never exceeds it)
+  const double eps_imag = std::max(std::pow(2.0, -20), vmax * 1.01);
+  set_scalars(P, k_bg, eps_imag, wl);
+  const int n3[3] = {P->dims.nx, P->dims.ny, P->dims.nz};
+  DevBuf* fb[3] = {&P->fx, &P->fy, &P->fz};
+  const double* fh[3] = {fx, fy, fz};
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> ones(n3[a], 1.0);
+    FM_CK(fb[a]->ensure(n3[a] * sizeof(double)));
+    FM_CK(cudaMemcpyAsync(fb[a]->p, fh[a] ? fh[a] : ones.data(), n3[a] * sizeof(double), cudaMemcpyHostToDevice, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+  }
+  FM_CK(P->V.ensure((size_t)P->n * P->esz));
+  k_potential_build<R><<<1184, 256, 0, P->st>>>(P->pi, (const double2*)P->eps_dev.p, eps_bg, k2, eps_imag,
+                                                (const double*)P->fx.p, (const double*)P->fy.p, (const double*)P->fz.p,
+                                                1.0 / P->kref2, (cplx<R>*)P->V.p);
+  FM_CK(cudaGetLastError());
+  int bornmax;
+  if (itmax < 0) {
+    const double steps = std::abs(2.0 * k_bg / eps_imag);
+    double ext = 0.0;
+    for (int a = 0; a < 3; ++a) ext += std::pow(n3[a] * P->desc.resolution[a], 2);
+    ext = std::sqrt(ext);
+    const int opt = (int)std::ceil(ext / steps / 2.0 + 1.0) * 2;
+    bornmax = opt * std::abs(itmax);
+  } else {
+    bornmax = itmax;
+  }
+  P->bornmax = bornmax;
+  FM_CK(cudaStreamSynchronize(P->st));
+  P->have_pot = true;
+  if (info) {
+    info->eps_imag = eps_imag;
+    info->k_bg = k_bg;
+    info->bornmax = bornmax;
+  }
+  return FM_OK;
+}
+
+fm_status fm_build_potential(fm_plan* P, const double* eps, double eps_bg, double wl, const double* fx, const double* fy,
+                             const double* fz, int itmax, fm_potential_info* info) {
+  FM_TRY(check_plan(P, 1, false));
+  if (!eps) return fail(FM_ERR_INVALID, "null permittivity");
+  if (!(eps_bg > 0)) return fail(FM_ERR_INVALID, "permittivity_bg must be positive");
+  if (!(wl > 0)) return fail(FM_ERR_INVALID, "wavelength must be positive");
+  return P->prec == FM_PREC_F64 ? build_potential_t<double>(P, eps, eps_bg, wl, fx, fy, fz, itmax, info)
+                                : build_potential_t<float>(P, eps, eps_bg, wl, fx, fy, fz, itmax, info);
+}
+
+// plane-wave tables (FP64) for nrhs right-hand sides, following generate_incident_field
+static fm_status upload_waves(fm_plan* P, int nrhs, const int* first, const fm_plane_wave* src, double eps_bg) {
+  const int ns = first[nrhs];
+  const int n3[3] = {P->dims.nx, P->dims.ny, P->dims.nz};
+  const int g3[3] = {P->pi.gx, P->pi.gy, P->pi.gz};
+  const int p3[3] = {P->pi.px, P->pi.py, P->pi.pz};
+  std::vector<double2> tx((size_t)ns * n3[0]), ty((size_t)ns * n3[1]), tz((size_t)ns * n3[2]), pe(ns * 3), ph(ns * 3);
+  for (int s = 0; s < ns; ++s) {
+    const fm_plane_wave& w = src[s];
+    if (!(w.wavelength > 0)) return fail(FM_ERR_INVALID, "wavelength must be positive");
+    if (!(w.amplitude >= 0)) return fail(FM_ERR_INVALID, "amplitude must be non-negative");
+    const double k0 = 2.0 * M_PI / w.wavelength;
+    const double kb = k0 * std::sqrt(eps_bg);
+    double kn = std::sqrt(w.k_vector[0] * w.k_vector[0] + w.k_vector[1] * w.k_vector[1] + w.k_vector[2] * w.k_vector[2]);
+    if (!(std::abs(kn - 1.0) < 1e-10)) return fail(FM_ERR_INVALID, "k_vector must be normalized (|k| = 1)");
+    double kh[3];
+    for (int a = 0; a < 3; ++a) kh[a] = w.k_vector[a] / kn;
+    cd p[3];
+    for (int a = 0; a < 3; ++a) p[a] = cd(w.polarization[2 * a], w.polarization[2 * a + 1]);
+    cd edotk = std::conj(p[0]) * kh[0] + std::conj(p[1]) * kh[1] + std::conj(p[2]) * kh[2];
+    if (!(std::abs(edotk.real()) < 1e-10)) return fail(FM_ERR_INVALID, "polarization must be transverse to k_vector");
+    double pn = std::sqrt(std::norm(p[0]) + std::norm(p[1]) + std::norm(p[2]));
+    cd e0[3];
+    for (int a = 0; a < 3; ++a) e0[a] = p[a] / pn;
+    cd d = std::conj(e0[0]) * kh[0] + std::conj(e0[1]) * kh[1] + std::conj(e0[2]) * kh[2];
+    cd ep[3];
+    for (int a = 0; a < 3; ++a) ep[a] = e0[a] - d * kh[a];
+    double en = std::sqrt(std::norm(ep[0]) + std::norm(ep[1]) + std::norm(ep[2]));
+    for (int a = 0; a < 3; ++a) ep[a] /= en;
+    const double zimp = 377.0 / std::sqrt(eps_bg);
+    cd hp[3] = {(kh[1] * ep[2] - kh[2] * ep[1]) / zimp, (kh[2] * ep[0] - kh[0] * ep[2]) / zimp,
+                (kh[0] * ep[1] - kh[1] * ep[0]) / zimp};
+    for (int a = 0; a < 3; ++a) {
+      pe[s * 3 + a] = make_double2(ep[a].real(), ep[a].imag());
+      ph[s * 3 + a] = make_double2(hp[a].real(), hp[a].imag());
+    }
+    std::vector<double2>* tabs[3] = {&tx, &ty, &tz};
+    for (int a = 0; a < 3; ++a) {
+      const double center = (g3[a] - 1) * P->desc.resolution[a] / 2.0;
+      for (int i = 0; i < n3[a]; ++i) {
+        const double r = (double)(i - p3[a]) * P->desc.resolution[a] - center;
+        double ph_ = kb * kh[a] * r;
+        cd v = std::exp(cd(0.0, ph_));
+        if (a == 2) v *= w.amplitude * std::exp(cd(0.0, w.phase));
+        (*tabs[a])[(size_t)s * n3[a] + i] = make_double2(v.real(), v.imag());
+      }
+    }
+  }
+  auto up = [&](DevBuf& b, const void* h, size_t bytes) -> fm_status {
+    FM_CK(b.ensure(std::max<size_t>(bytes, 16)));
+    FM_CK(cudaMemcpyAsync(b.p, h, bytes, cudaMemcpyHostToDevice, P->st));
+    return FM_OK;
+  };
+  FM_TRY(up(P->wt_x, tx.data(), tx.size() * sizeof(double2)));
+  FM_TRY(up(P->wt_y, ty.data(), ty.size() * sizeof(double2)));
+  FM_TRY(up(P->wt_z, tz.data(), tz.size() * sizeof(double2)));
+  FM_TRY(up(P->wt_pe, pe.data(), pe.size() * sizeof(double2)));
+  FM_TRY(up(P->wt_ph, ph.data(), ph.size() * sizeof(double2)));
+  FM_TRY(up(P->wt_first, first, (nrhs + 1) * sizeof(int)));
+  FM_CK(cudaStreamSynchronize(P->st));
+  return FM_OK;
+}
+
+template <typename R>
+static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_plane_wave* src, double eps_bg,
+                               const fm_solve_opts& o, double* E, double* H, fm_solve_info* info) {
+  int wave = 1;
+  FM_TRY(plan_wave_size<R>(P, nrhs, o, wave));
+  const long long g = (long long)P->pi.gx * P->pi.gy * P->pi.gz;
+  const bool keep = (E == nullptr);
+  if (keep) {
+    FM_CK(P->Eo.ensure((size_t)nrhs * 3 * g * sizeof(double2)));
+    FM_CK(P->Ho.ensure((size_t)nrhs * 3 * g * sizeof(double2)));
+  } else {
+    FM_CK(P->Eo.ensure((size_t)wave * 3 * g * sizeof(double2)));
+    FM_CK(P->Ho.ensure((size_t)wave * 3 * g * sizeof(double2)));
+  }
+  bool all_ok = true;
+  for (int b0 = 0; b0 < nrhs; b0 += wave) {
+    const int nb = std::min(wave, nrhs - b0);
+    std::vector<int> f(nb + 1);
+    for (int b = 0; b <= nb; ++b) f[b] = first[b0 + b] - first[b0];
+    FM_TRY(upload_waves(P, nb, f.data(), src + first[b0], eps_bg));
+    FM_CK(P->sbuf.ensure((size_t)nb * P->M * sizeof(cplx<R>)));
+    WaveTabs wt{(const double2*)P->wt_x.p, (const double2*)P->wt_y.p, (const double2*)P->wt_z.p,
+                (const double2*)P->wt_pe.p, (const double2*)P->wt_ph.p, (const int*)P->wt_first.p};
+    k_source_term<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->V.p, P->eps_imag / P->kref2,
+                                                       (cplx<R>*)P->sbuf.p, nullptr);
+    FM_CK(cudaGetLastError());
+    std::vector<fm_solve_info> inf(nb);
+    FM_TRY(solve_core<R>(P, nb, o, inf));
+    double2* eo = (double2*)P->Eo.p + (keep ? (size_t)b0 * 3 * g : 0);
+    double2* ho = (double2*)P->Ho.p + (keep ? (size_t)b0 * 3 * g : 0);
+    k_assemble<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->xbuf.p,
+                                                    (const cplx<R>*)P->ebuf.p, eo, ho);
+    FM_CK(cudaGetLastError());
+    if (!keep) {
+      FM_CK(cudaMemcpyAsync(E + (size_t)b0 * 3 * g * 2, eo, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+      FM_CK(cudaMemcpyAsync(H + (size_t)b0 * 3 * g * 2, ho, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    }
+    FM_CK(cudaStreamSynchronize(P->st));
+    for (int b = 0; b < nb; ++b) {
+      if (info) info[b0 + b] = inf[b];
+      all_ok &= inf[b].solved != 0;
+    }
+  }
+  P->out_nrhs = keep ? nrhs : 0;
+  if (!all_ok) return fail(FM_NOT_CONVERGED, "iteration limit reached before the tolerance was met");
+  return FM_OK;
+}
+
+fm_status fm_solve_plane_waves(fm_plan* P, int nrhs, const int* first, const fm_plane_wave* sources, double eps_bg,
+                               const fm_solve_opts* opts, double* E, double* H, fm_solve_info* info) {
+  FM_TRY(check_plan(P, nrhs, true));
+  FM_TRY(validate_opts(opts));
+  if (!first || !sources) return fail(FM_ERR_INVALID, "null sources");
+  if ((E == nullptr) != (H == nullptr)) return fail(FM_ERR_INVALID, "E_out and H_out must both be set or both be NULL");
+  if (first[0] != 0) return fail(FM_ERR_INVALID, "first[0] must be 0");
+  for (int b = 0; b < nrhs; ++b)
+    if (first[b + 1] <= first[b]) return fail(FM_ERR_INVALID, "sources vector cannot be empty");
+  for (int b = 0; b < nrhs; ++b) {
+    for (int s = first[b] + 1; s < first[b + 1]; ++s)
+      if (sources[s].wavelength != sources[first[b]].wavelength)
+        return fail(FM_ERR_INVALID, "All sources must have the same wavelength for coherent superposition");
+    if (std::abs(sources[first[b]].wavelength - P->wavelength) > 1e-12 * P->wavelength)
+      return fail(FM_ERR_INVALID, "source wavelength differs from the wavelength of the potential");
+  }
+  if (!(eps_bg > 0)) return fail(FM_ERR_INVALID, "permittivity_bg must be positive");
+  return P->prec == FM_PREC_F64 ? solve_waves_t<double>(P, nrhs, first, sources, eps_bg, *opts, E, H, info)
+                                : solve_waves_t<float>(P, nrhs, first, sources, eps_bg, *opts, E, H, info);
+}
+
+fm_status fm_copy_fields(fm_plan* P, int nrhs, double* E, double* H) {
+  FM_TRY(check_plan(P, nrhs, false));
+  if (!E || !H) return fail(FM_ERR_INVALID, "null buffer");
+  if (nrhs > P->out_nrhs) return fail(FM_ERR_INVALID, "fewer fields are resident than requested");
+  const long long g = (long long)P->pi.gx * P->pi.gy * P->pi.gz;
+  FM_CK(cudaMemcpyAsync(E, P->Eo.p, (size_t)nrhs * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaMemcpyAsync(H, P->Ho.p, (size_t)nrhs * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  return FM_OK;
+}
+

@@ -1,0 +1,32 @@
+// Host-side launchers of the axis passes (implemented per precision in
+// fm_pass_f32.cu / fm_pass_f64.cu so the two instantiation sets compile in parallel).
+#pragma once
+#include <cuda_runtime.h>
+#include "fm_passes.cuh"
+
+namespace fm {
+
+// Largest supported axis length and the largest z length with the averaged
+// (length-2L) transform.
+constexpr int AXIS_MAX = 512;
+constexpr int AXIS_MAX_AVG2 = 256;
+
+template <typename R>
+cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, const double* rhs_scale, const void* twx,
+                      const void* rampx, void* out, const int* active, cudaStream_t st);
+template <typename R>
+cudaError_t launch_y(const Dims& d, int dir, const void* in, const void* twy, const void* rampy, void* out,
+                     const int* active, cudaStream_t st);
+template <typename R>
+cudaError_t launch_zg(const Dims& d, int mode, const void* in, const GreenParams& gp, const void* twz, const void* rz,
+                      void* out, const int* active, cudaStream_t st);
+template <typename R>
+cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
+                      const double* rhs_scale, const EpiParams& ep, const void* twx, const void* rampx, void* out,
+                      const int* active, cudaStream_t st);
+
+// pencils that share one warp for an axis of length L (y/z passes need nx to be a multiple)
+template <typename R>
+int pencils_per_warp(int L);
+
+}  // namespace fm

@@ -1,0 +1,378 @@
+// Axis passes of the dyadic-Green convolution and of the spectral curl.
+//
+// Field layout (column-major like the reference): element (x, y, z, c, b) of a
+// batch of 3-component fields sits at x + nx*(y + ny*(z + nz*(c + 3*b))).
+// One Green application G_avg(V.*x) runs as five passes, each reading and
+// writing the batch once:
+//   XF  x-rows   : psi = V.*x (prologue) -> forward FFT along x
+//   YF  y-pencils: forward FFT along y
+//   ZG  z-pencils: forward FFT along z -> 3x3 dyadic Green -> inverse FFT along z
+//                  (both sub-pixel-shifted branches of the reference's average are
+//                   produced by ONE length-2L transform of the zero-padded pencil)
+//   YI  y-pencils: inverse FFT along y
+//   XI  x-rows   : inverse FFT along x -> epilogue (operator / preconditioner / residual)
+// Every pass keeps a pencil in registers (see fm_fft.cuh); warps are independent.
+#pragma once
+#include "fm_fft.cuh"
+
+namespace fm {
+
+struct Dims {
+  int nx, ny, nz, nb;
+  long long n;  // nx*ny*nz
+};
+
+// Warp-local exchange buffers: each warp owns P pencils x SmemLen<L>.
+template <typename T, int LFFT>
+__device__ __forceinline__ T* warp_smem(T* base, int warp_in_cta, int pencils_per_warp, int p) {
+  return base + ((size_t)warp_in_cta * pencils_per_warp + p) * SmemLen<LFFT>::v;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_table(T* dst, const T* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// XF: prologue + forward FFT along x.  One warp = P rows (y,z,b); a thread
+// handles all 3 components of its row so V is loaded once.
+// PRO: 0 copy, 1 multiply by V, 2 multiply by V and by a per-RHS real scale.
+// ---------------------------------------------------------------------------
+enum { PRO_COPY = 0, PRO_V = 1, PRO_V_SCALE = 2 };
+
+template <typename R, int L, int PRO>
+__global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ V,
+                                            const double* __restrict__ rhs_scale, const cplx<R>* __restrict__ twx,
+                                            const cplx<R>* __restrict__ rampx, cplx<R>* __restrict__ out,
+                                            const int* __restrict__ active) {
+  using T = cplx<R>;
+  using P_ = Plan<L, R>;
+  constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* ex = tw + L;
+  load_table(tw, twx, L);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
+  const int p = lane / TP, t = lane % TP;
+  const long long rows = (long long)d.ny * d.nz * d.nb;
+  const long long row = ((long long)blockIdx.x * (blockDim.x >> 5) + wic) * PW + p;
+  if (row >= rows) return;  // whole pencils exit together (rows is a multiple of PW)
+  const int b = (int)(row / ((long long)d.ny * d.nz));
+  if (active && !active[b]) return;
+  const long long yz = row - (long long)b * d.ny * d.nz;
+  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T vrow[E];
+  if constexpr (PRO != PRO_COPY) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) vrow[e] = V[yz * L + lay_idx<L, E, P_::R0>(t, e)];
+  }
+  R s = R(1);
+  if constexpr (PRO == PRO_V_SCALE) s = (R)rhs_scale[b];
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
+    T v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int x = lay_idx<L, E, P_::R0>(t, e);
+      T a = in[base + x];
+      if constexpr (PRO != PRO_COPY) a = cmul(a, vrow[e]);
+      if constexpr (PRO == PRO_V_SCALE) a = cscale(a, s);
+      if (rampx) a = cmul(a, rampx[x]);
+      v[e] = a;
+    }
+    fft_fwd_plan<-1, P_>(v, sm, tw, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) out[base + lay_idx<L, E, P_::RL>(t, e)] = v[e];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Y pass (forward DIR=-1 or inverse DIR=+1), plain.  One warp = P consecutive
+// x columns at fixed (z, c, b); lane = t*P + p so consecutive lanes read
+// consecutive x.
+// ---------------------------------------------------------------------------
+template <typename R, int L, int DIR>
+__global__ void __launch_bounds__(256) k_y(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ twy,
+                                           const cplx<R>* __restrict__ rampy, cplx<R>* __restrict__ out,
+                                           const int* __restrict__ active) {
+  using T = cplx<R>;
+  using P_ = Plan<L, R>;
+  constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* ex = tw + L;
+  load_table(tw, twy, L);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
+  const int p = lane % PW, t = lane / PW;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wic;
+  const int xg = d.nx / PW;
+  const long long total = (long long)xg * d.nz * 3 * d.nb;
+  if (gw >= total) return;
+  const int x = (int)(gw % xg) * PW + p;
+  const long long zcb = gw / xg;  // z + nz*(c + 3b)
+  const int b = (int)(zcb / (3LL * d.nz));
+  if (active && !active[b]) return;
+  const long long base = zcb * (long long)d.ny * d.nx + x;
+  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T v[E];
+  if constexpr (DIR < 0) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int y = lay_idx<L, E, P_::R0>(t, e);
+      T a = in[base + (long long)y * d.nx];
+      if (rampy) a = cmul(a, rampy[y]);
+      v[e] = a;
+    }
+    fft_fwd_plan<-1, P_>(v, sm, tw, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) out[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx] = v[e];
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = in[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx];
+    fft_rev_plan<+1, P_>(v, sm, tw, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int y = lay_idx<L, E, P_::R0>(t, e);
+      T a = v[e];
+      if (rampy) a = cmul(a, cconj(rampy[y]));
+      out[base + (long long)y * d.nx] = a;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Z pass with the dyadic Green (or the curl) between forward and inverse FFT.
+// MODE_AVG2 : the reference's average of the +s and -s shifted Green functions
+//             (s = 1/4 on z).  The pencil psi(z), z < L, is multiplied by
+//             exp(-i*pi*z/(2L)), zero-padded to 2L and transformed; bin 2k holds
+//             the +s spectrum at k and bin 2k-1 the -s spectrum at k (mod L).
+//             After the Green product per bin, the length-2L inverse transform,
+//             restricted to z < L and multiplied by exp(+i*pi*z/(2L)), is
+//             L*(o_plus + o_minus) up to the constant folded into `scale`.
+// MODE_ONE  : one branch with shift sz (0 when z is periodic), ramp table rz.
+// MODE_CURL : ik x E with the curl k-index, complex scale folded in.
+// ---------------------------------------------------------------------------
+enum { ZMODE_AVG2 = 0, ZMODE_ONE = 1, ZMODE_CURL = 2 };
+
+struct GreenParams {
+  double dk[3];      // 2*pi/(N_d*res_d) / k_ref
+  double shift[3];   // sub-pixel shift of this branch per axis (x, y used in all modes)
+  double ksq_re, ksq_im;  // k_square / k_ref^2
+  double scale_re, scale_im;  // folded normalisation (and curl factor)
+  int curl_index;    // 1 -> curl index formula for odd sizes
+};
+
+template <typename R>
+__device__ __forceinline__ R kidx_green(int i, int n) {
+  const int h = n >> 1;
+  return (R)(((i + h) % n) - h);
+}
+template <typename R>
+__device__ __forceinline__ R kidx_curl(int i, int n) {
+  return (R)(i < (n >> 1) ? i : i - n);
+}
+
+template <typename R, int L, int MODE>
+__global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<R>* __restrict__ in, GreenParams gp,
+                                            const cplx<R>* __restrict__ twz, const cplx<R>* __restrict__ rz,
+                                            cplx<R>* __restrict__ out, const int* __restrict__ active) {
+  using T = cplx<R>;
+  constexpr int LF = (MODE == ZMODE_AVG2) ? 2 * L : L;
+  using P_ = Plan<LF, R>;
+  constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* rtab = tw + LF;
+  T* ex = rtab + L;
+  load_table(tw, twz, LF);
+  if (rz) load_table(rtab, rz, L);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
+  const int p = lane % PW, t = lane / PW;
+  const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wic;
+  const int xg = d.nx / PW;
+  const long long total = (long long)xg * d.ny * d.nb;
+  if (gw >= total) return;
+  const int x = (int)(gw % xg) * PW + p;
+  const long long yb = gw / xg;
+  const int y = (int)(yb % d.ny);
+  const int b = (int)(yb / d.ny);
+  if (active && !active[b]) return;
+  const long long plane = (long long)d.nx * d.ny;
+  const long long base0 = (long long)b * 3 * d.n + (long long)y * d.nx + x;
+  T* sm = warp_smem<T, LF>(ex, wic, PW, p);
+
+  T v[3][E];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int z = lay_idx<LF, E, P_::R0>(t, e);
+      T a = czero<T>();
+      if (MODE != ZMODE_AVG2 || z < L) {
+        a = in[base0 + (long long)c * d.n + (long long)z * plane];
+        if (MODE != ZMODE_CURL && rz) a = cmul(a, rtab[z]);
+      }
+      v[c][e] = a;
+    }
+    fft_fwd_plan<-1, P_>(v[c], sm, tw, t);
+    __syncwarp();
+  }
+
+  // per-bin 3x3 operator
+  {
+    int kxi = x, kyi = y;
+    R kx, ky;
+    if (MODE == ZMODE_CURL) {
+      kx = (R)gp.dk[0] * kidx_curl<R>(kxi, d.nx);
+      ky = (R)gp.dk[1] * kidx_curl<R>(kyi, d.ny);
+    } else {
+      kx = (R)gp.dk[0] * (kidx_green<R>(kxi, d.nx) + (R)gp.shift[0]);
+      ky = (R)gp.dk[1] * (kidx_green<R>(kyi, d.ny) + (R)gp.shift[1]);
+    }
+    const R ksr = (R)gp.ksq_re, ksi = (R)gp.ksq_im;
+    const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
+    // 1/k_square
+    const R kden = ksr * ksr + ksi * ksi;
+    const T iks = mk(ksr / kden, -ksi / kden);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int m = lay_idx<LF, E, P_::RL>(t, e);
+      R kz;
+      if constexpr (MODE == ZMODE_AVG2) {
+        if ((m & 1) == 0) kz = (R)gp.dk[2] * (kidx_green<R>(m >> 1, L) + (R)gp.shift[2]);
+        else kz = (R)gp.dk[2] * (kidx_green<R>(((m + 1) >> 1) % L, L) - (R)gp.shift[2]);
+      } else if constexpr (MODE == ZMODE_ONE) {
+        kz = (R)gp.dk[2] * (kidx_green<R>(m, L) + (R)gp.shift[2]);
+      } else {
+        kz = (R)gp.dk[2] * kidx_curl<R>(m, L);
+      }
+      T e1 = v[0][e], e2 = v[1][e], e3 = v[2][e];
+      if constexpr (MODE == ZMODE_CURL) {
+        // (ik x E) * sc
+        T c1 = csub(cscale(e3, ky), cscale(e2, kz));
+        T c2 = csub(cscale(e1, kz), cscale(e3, kx));
+        T c3 = csub(cscale(e2, kx), cscale(e1, ky));
+        const T isc = cmul_i<1>(sc);
+        v[0][e] = cmul(c1, isc);
+        v[1][e] = cmul(c2, isc);
+        v[2][e] = cmul(c3, isc);
+      } else {
+        T kE = cadd(cadd(cscale(e1, kx), cscale(e2, ky)), cscale(e3, kz));
+        kE = cmul(kE, iks);
+        const R k2 = kx * kx + ky * ky + kz * kz;
+        const R dr = k2 - ksr, di = -ksi;
+        const R dd = dr * dr + di * di;
+        const T f = cmul(sc, mk(dr / dd, -di / dd));
+        v[0][e] = cmul(csub(e1, cscale(kE, kx)), f);
+        v[1][e] = cmul(csub(e2, cscale(kE, ky)), f);
+        v[2][e] = cmul(csub(e3, cscale(kE, kz)), f);
+      }
+    }
+  }
+
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    fft_rev_plan<+1, P_>(v[c], sm, tw, t);
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int z = lay_idx<LF, E, P_::R0>(t, e);
+      if (MODE != ZMODE_AVG2 || z < L) {
+        T a = v[c][e];
+        if (MODE != ZMODE_CURL && rz) a = cmul(a, cconj(rtab[z]));
+        out[base0 + (long long)c * d.n + (long long)z * plane] = a;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// XI: inverse FFT along x + epilogue.
+//   EPI_STORE    out = g
+//   EPI_OP       out = beta*out + alpha*(x - g)                 (CBSLinearOperator)
+//   EPI_PREC_OP  out = (i/eps)*V*(xs - g)                       (M^{-1} A x)
+//   EPI_PREC_RES out = (i/eps)*V*(bb - xs + g)                  (M^{-1}(b - A x))
+// xs = x * rhs_scale[b] when rhs_scale is given.
+// ---------------------------------------------------------------------------
+enum { EPI_STORE = 0, EPI_OP = 1, EPI_PREC_OP = 2, EPI_PREC_RES = 3 };
+
+struct EpiParams {
+  double alpha_re, alpha_im, beta_re, beta_im;
+  double inv_eps;  // 1/eps_imag (scaled units)
+};
+
+template <typename R, int L, int EPI>
+__global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ V,
+                                            const cplx<R>* __restrict__ xv, const cplx<R>* __restrict__ bv,
+                                            const double* __restrict__ rhs_scale, EpiParams ep,
+                                            const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ rampx,
+                                            cplx<R>* __restrict__ out, const int* __restrict__ active) {
+  using T = cplx<R>;
+  using P_ = Plan<L, R>;
+  constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* tw = reinterpret_cast<T*>(smraw);
+  T* ex = tw + L;
+  load_table(tw, twx, L);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
+  const int p = lane / TP, t = lane % TP;
+  const long long rows = (long long)d.ny * d.nz * d.nb;
+  const long long row = ((long long)blockIdx.x * (blockDim.x >> 5) + wic) * PW + p;
+  if (row >= rows) return;
+  const int b = (int)(row / ((long long)d.ny * d.nz));
+  if (active && !active[b]) return;
+  const long long yz = row - (long long)b * d.ny * d.nz;
+  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T gam[E];
+  if constexpr (EPI == EPI_PREC_OP || EPI == EPI_PREC_RES) {
+    const R ie = (R)ep.inv_eps;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      T vv = V[yz * L + lay_idx<L, E, P_::R0>(t, e)];
+      gam[e] = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
+    }
+  }
+  R s = R(1);
+  if (rhs_scale) s = (R)rhs_scale[b];
+  const T al = mk((R)ep.alpha_re, (R)ep.alpha_im), be = mk((R)ep.beta_re, (R)ep.beta_im);
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
+    T v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = in[base + lay_idx<L, E, P_::RL>(t, e)];
+    fft_rev_plan<+1, P_>(v, sm, tw, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int x = lay_idx<L, E, P_::R0>(t, e);
+      const long long ix = base + x;
+      T g = v[e];
+      if (rampx) g = cmul(g, cconj(rampx[x]));
+      T r;
+      if constexpr (EPI == EPI_STORE) {
+        r = g;
+      } else if constexpr (EPI == EPI_OP) {
+        T xx = xv[ix];
+        T a = cmul(al, csub(xx, g));
+        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, out[ix]));
+        r = a;
+      } else if constexpr (EPI == EPI_PREC_OP) {
+        T xx = cscale(xv[ix], s);
+        r = cmul(gam[e], csub(xx, g));
+      } else {
+        T xx = cscale(xv[ix], s);
+        r = cmul(gam[e], cadd(csub(bv[ix], xx), g));
+      }
+      out[ix] = r;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace fm

@@ -1,0 +1,125 @@
+"""ctypes binding of libfmcuda (declarations in include/fmcuda.h).
+
+The shared library is built in-tree next to this file (see ``build.py``).  There
+is no CPU fallback: importing the solver without the library, or calling it on a
+machine without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import warnings
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfmcuda.so")
+
+FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_NOT_CONVERGED, FM_ERR_NONFINITE, FM_ERR_TIMEOUT, FM_ERR_CUDA, \
+    FM_ERR_UNSUPPORTED = range(8)
+FM_PREC_F64, FM_PREC_F32 = 0, 1
+FM_METHOD_GMRES, FM_METHOD_BICGSTAB, FM_METHOD_RICHARDSON = 0, 1, 2
+FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2 = 0, 1, 2
+
+STATUS_NAMES = {
+    FM_OK: "FM_OK", FM_ERR_INVALID: "FM_ERR_INVALID", FM_ERR_OOM: "FM_ERR_OOM",
+    FM_NOT_CONVERGED: "FM_NOT_CONVERGED", FM_ERR_NONFINITE: "FM_ERR_NONFINITE",
+    FM_ERR_TIMEOUT: "FM_ERR_TIMEOUT", FM_ERR_CUDA: "FM_ERR_CUDA", FM_ERR_UNSUPPORTED: "FM_ERR_UNSUPPORTED",
+}
+
+# Every symbol the header declares; tests check the library exports all of them.
+EXPORTED = (
+    "fm_abi_version", "fm_last_error", "fm_device_count", "fm_plan_create", "fm_plan_destroy", "fm_plan_bytes",
+    "fm_set_potential", "fm_green_apply", "fm_apply_operator", "fm_apply_preconditioner", "fm_curl_field",
+    "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
+)
+
+
+class fm_plan_desc(C.Structure):
+    _fields_ = [("grid", C.c_int * 3), ("pad", C.c_int * 3), ("resolution", C.c_double * 3),
+                ("absorbing", C.c_int * 3), ("precision", C.c_int), ("max_rhs", C.c_int), ("device", C.c_int)]
+
+
+class fm_solve_opts(C.Structure):
+    _fields_ = [("method", C.c_int), ("ortho", C.c_int), ("restart", C.c_int), ("maxiters", C.c_int),
+                ("reltol", C.c_double), ("abstol", C.c_double), ("timeout_s", C.c_double)]
+
+
+class fm_solve_info(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("solved", C.c_int), ("residual", C.c_double),
+                ("residual0", C.c_double)]
+
+
+class fm_potential_info(C.Structure):
+    _fields_ = [("eps_imag", C.c_double), ("k_bg", C.c_double), ("bornmax", C.c_int)]
+
+
+class fm_plane_wave(C.Structure):
+    _fields_ = [("wavelength", C.c_double), ("polarization", C.c_double * 6), ("k_vector", C.c_double * 3),
+                ("amplitude", C.c_double), ("phase", C.c_double)]
+
+
+class FMError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libfmcuda.so once; raise loudly if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libfmcuda.so not found at {LIB_PATH}; build it with "
+                          f"`python -c 'import __graft_entry__ as g; g.build()'` or `make -C csrc`")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    D = C.POINTER(C.c_double)
+    L.fm_abi_version.restype = C.c_int
+    L.fm_last_error.restype = C.c_char_p
+    L.fm_device_count.restype = C.c_int
+    L.fm_plan_create.argtypes = [C.POINTER(fm_plan_desc), C.POINTER(P)]
+    L.fm_plan_destroy.argtypes = [P]
+    L.fm_plan_destroy.restype = None
+    L.fm_plan_bytes.argtypes = [C.POINTER(fm_plan_desc), C.c_int, C.c_int]
+    L.fm_plan_bytes.restype = C.c_longlong
+    L.fm_set_potential.argtypes = [P, P, C.c_double, C.c_double, C.c_double]
+    L.fm_green_apply.argtypes = [P, C.c_int, P, P]
+    L.fm_apply_operator.argtypes = [P, C.c_int, P, P, C.c_double, C.c_double, C.c_double, C.c_double]
+    L.fm_apply_preconditioner.argtypes = [P, C.c_int, P, P]
+    L.fm_curl_field.argtypes = [P, C.c_int, P, P]
+    L.fm_solve_source.argtypes = [P, C.c_int, P, C.POINTER(fm_solve_opts), P, P, C.POINTER(fm_solve_info)]
+    L.fm_build_potential.argtypes = [P, P, C.c_double, C.c_double, P, P, P, C.c_int, C.POINTER(fm_potential_info)]
+    L.fm_solve_plane_waves.argtypes = [P, C.c_int, C.POINTER(C.c_int), C.POINTER(fm_plane_wave), C.c_double,
+                                       C.POINTER(fm_solve_opts), P, P, C.POINTER(fm_solve_info)]
+    L.fm_copy_fields.argtypes = [P, C.c_int, P, P]
+    L.fm_synchronize.argtypes = [P]
+    for name in ("fm_plan_create", "fm_set_potential", "fm_green_apply", "fm_apply_operator",
+                 "fm_apply_preconditioner", "fm_curl_field", "fm_solve_source", "fm_build_potential",
+                 "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(status: int, allow_not_converged: bool = False) -> int:
+    """Raise FMError for a failing status; FM_NOT_CONVERGED passes when allowed (the reference warns)."""
+    if status == FM_OK:
+        return status
+    if status == FM_NOT_CONVERGED and allow_not_converged:
+        return status
+    msg = lib().fm_last_error().decode(errors="replace")
+    if status == FM_ERR_INVALID:
+        raise ValueError(msg)
+    raise FMError(status, msg)
+
+
+def ptr(a) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+def warn_not_converged():
+    # convergent_born.jl:753-755
+    warnings.warn("LinearSolve.jl did not converge.", RuntimeWarning, stacklevel=3)

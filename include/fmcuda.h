@@ -1,0 +1,163 @@
+/* fmcuda.h -- C ABI of libfmcuda, the B200 (sm_100a) convergent Born series solver.
+ *
+ * The library replaces the device path of FrequencyMaxwell.jl's
+ * solve(solver::ConvergentBornSolver, sources, medium): the KernelAbstractions
+ * kernels, the FFTW/CUFFT transforms and the LinearSolve/Krylov loop.  Host code
+ * (Julia via ccall, Python via ctypes) keeps the reference API and calls these
+ * entry points.  Each function names the reference code it stands in for
+ * (paths inside the FrequencyMaxwell.jl project).
+ *
+ * Conventions
+ *   - Complex arrays cross the ABI as interleaved FP64 (re, im) pairs.
+ *   - Fields are column-major (Nx', Ny', Nz', 3) per right-hand side (RHS), x
+ *     fastest, components planar, RHS outermost: element (x,y,z,c,b) at
+ *     x + Nx'*(y + Ny'*(z + Nz'*(c + 3*b))).  Nx', Ny', Nz' are the padded sizes.
+ *   - A plan owns all device memory and one CUDA stream.  Plans are not
+ *     thread-safe; different plans may be used from different host threads.
+ *   - Every entry point returns an fm_status; fm_last_error() gives a message
+ *     for the calling thread.  Non-convergence returns FM_NOT_CONVERGED with the
+ *     result still written (the reference only warns:
+ *     src/solvers/convergent_born.jl:753-755).
+ */
+#ifndef FMCUDA_H
+#define FMCUDA_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMCUDA_ABI_VERSION 1
+
+typedef enum {
+  FM_OK = 0,
+  FM_ERR_INVALID = 1,      /* bad argument (reference: ArgumentError) */
+  FM_ERR_OOM = 2,          /* device allocation failed */
+  FM_NOT_CONVERGED = 3,    /* iteration limit reached; outputs written */
+  FM_ERR_NONFINITE = 4,    /* NaN/Inf found in an input or a result */
+  FM_ERR_TIMEOUT = 5,      /* host-side deadline passed */
+  FM_ERR_CUDA = 6,         /* CUDA runtime error */
+  FM_ERR_UNSUPPORTED = 7   /* size or option this build does not support */
+} fm_status;
+
+enum { FM_PREC_F64 = 0, FM_PREC_F32 = 1 };
+enum { FM_METHOD_GMRES = 0, FM_METHOD_BICGSTAB = 1, FM_METHOD_RICHARDSON = 2 };
+enum { FM_ORTHO_MGS = 0, FM_ORTHO_CGS = 1, FM_ORTHO_CGS2 = 2 };
+
+typedef struct fm_plan fm_plan;
+
+/* Grid description.  Mirrors what ConvergentBornSolver derives from its
+ * boundary conditions: padding_pixels and subpixel_shift per axis
+ * (src/solvers/boundary_conditions.jl:450-527) and compute_ROI
+ * (src/solvers/convergent_born.jl:250-260). */
+typedef struct {
+  int grid[3];          /* unpadded (Nx, Ny, Nz) */
+  int pad[3];           /* padding pixels per side and axis */
+  double resolution[3]; /* voxel size in metres */
+  int absorbing[3];     /* 1: absorbing axis -> shift 0.25 and (G(+s)+G(-s))/2 averaging */
+  int precision;        /* FM_PREC_F64 or FM_PREC_F32 */
+  int max_rhs;          /* largest batch the plan will be asked to hold at once (>= 1) */
+  int device;           /* CUDA device ordinal */
+} fm_plan_desc;
+
+typedef struct {
+  int method;           /* FM_METHOD_* (reference default: GMRES, convergent_born.jl:197) */
+  int ortho;            /* FM_ORTHO_* for GMRES (Krylov.jl uses MGS) */
+  int restart;          /* 0: full GMRES as KrylovJL_GMRES runs it; m > 0: GMRES(m) */
+  int maxiters;         /* max(2*Bornmax, 100) in the reference (convergent_born.jl:746) */
+  double reltol;        /* solver.tolerance (convergent_born.jl:744) */
+  double abstol;        /* solver.tolerance * 1e-2 (convergent_born.jl:745) */
+  double timeout_s;     /* host-side deadline for the whole call, 0 = none */
+} fm_solve_opts;
+
+typedef struct {
+  int iterations;       /* Krylov iterations (sol.iters, convergent_born.jl:761-763) */
+  int solved;           /* 1 when the stopping test was met */
+  double residual;      /* last preconditioned residual estimate (sol.resid, :764-766) */
+  double residual0;     /* initial preconditioned residual norm */
+} fm_solve_info;
+
+typedef struct {
+  double eps_imag;      /* max(2^-20, 1.01 max|V|)   (convergent_born.jl:641) */
+  double k_bg;          /* 2 pi sqrt(eps_bg) / lambda (convergent_born.jl:630) */
+  int bornmax;          /* Bornmax (convergent_born.jl:653-660) */
+} fm_potential_info;
+
+/* One plane-wave source, as PlaneWaveSource holds it (src/sources/plane_wave.jl:63-116). */
+typedef struct {
+  double wavelength;
+  double polarization[6];  /* 3 complex values, interleaved (re, im) */
+  double k_vector[3];      /* unit propagation direction */
+  double amplitude;
+  double phase;
+} fm_plane_wave;
+
+int fm_abi_version(void);
+const char* fm_last_error(void);
+int fm_device_count(void);
+
+/* Plan lifetime.  Replaces the device-side state that ConvergentBornSolver and
+ * DyadicGreen allocate per solve (convergent_born.jl:619-675,
+ * src/core/dyadic_green.jl:67-99). */
+fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out);
+void fm_plan_destroy(fm_plan* plan);
+/* Device bytes a plan needs to hold `nrhs` right-hand sides with a Krylov basis of `basis` vectors. */
+long long fm_plan_bytes(const fm_plan_desc* desc, int nrhs, int basis);
+
+/* ---- reference seams (host buffers) ------------------------------------ */
+
+/* to_device(V) of _initialize_solver! (convergent_born.jl:649-650): the padded,
+ * attenuated potential including the -i*eps_imag shift, plus the scalars that
+ * the reference derives next to it. */
+fm_status fm_set_potential(fm_plan* plan, const double* V, double k_bg, double eps_imag, double wavelength);
+
+/* conv!(::DyadicGreen, x) (src/core/dyadic_green.jl:127-152), nrhs fields in, nrhs fields out. */
+fm_status fm_green_apply(fm_plan* plan, int nrhs, const double* x, double* y);
+
+/* mul!(y, ::CBSLinearOperator, x, alpha, beta): y = beta*y + alpha*(x - G_avg(V.*x))
+ * (convergent_born.jl:482-512). */
+fm_status fm_apply_operator(fm_plan* plan, int nrhs, const double* x, double* y, double alpha_re, double alpha_im,
+                            double beta_re, double beta_im);
+
+/* ldiv!(y, ::CBSPreconditioner, x): y = (i/eps_imag) .* V .* x (convergent_born.jl:398-410). */
+fm_status fm_apply_preconditioner(fm_plan* plan, int nrhs, const double* x, double* y);
+
+/* _compute_magnetic_field (convergent_born.jl:784-800 with src/core/curl.jl:55-116):
+ * H = -i*lambda/(2*pi*377) * curl(E). */
+fm_status fm_curl_field(fm_plan* plan, int nrhs, const double* E, double* H);
+
+/* _solve_cbs_scattering (convergent_born.jl:703-774): from source terms S (the
+ * reference's V.*E_inc + i*eps_imag.*E_inc, :585-586) to the scattered E and H on
+ * the padded grid.  info is an array of nrhs entries. */
+fm_status fm_solve_source(fm_plan* plan, int nrhs, const double* S, const fm_solve_opts* opts, double* E_scat,
+                          double* H_scat, fm_solve_info* info);
+
+/* ---- device-side set-up and assembly ----------------------------------- */
+
+/* The numerics of _initialize_solver! (convergent_born.jl:625-660) run on the
+ * device from the unpadded permittivity (Nx, Ny, Nz) complex array.  fx, fy, fz
+ * are the per-axis attenuation filters over the padded axes (all ones on
+ * periodic axes), as _apply_attenuation_to_potential! builds them
+ * (convergent_born.jl:893-944). */
+fm_status fm_build_potential(fm_plan* plan, const double* eps, double eps_bg, double wavelength, const double* fx,
+                             const double* fy, const double* fz, int iterations_max, fm_potential_info* info);
+
+/* The whole of solve(solver, sources, medium) after set-up (convergent_born.jl:576-599):
+ * incident plane waves (generate_incident_field, plane_wave.jl:198-268, coherent sum
+ * field_generation.jl:42-78), source term, CBS solve, magnetic field, incident
+ * addition and crop_to_ROI.  RHS b owns sources [first[b], first[b+1]).  E_out and
+ * H_out receive the cropped total fields (Nx, Ny, Nz, 3) per RHS; when they are
+ * NULL the fields stay on the device (see fm_copy_fields). */
+fm_status fm_solve_plane_waves(fm_plan* plan, int nrhs, const int* first, const fm_plane_wave* sources,
+                               double permittivity_bg, const fm_solve_opts* opts, double* E_out, double* H_out,
+                               fm_solve_info* info);
+
+/* Copy the cropped total fields of the last fm_solve_plane_waves call to the host. */
+fm_status fm_copy_fields(fm_plan* plan, int nrhs, double* E_out, double* H_out);
+
+/* Wait for the plan's stream. */
+fm_status fm_synchronize(fm_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMCUDA_H */
