@@ -1,0 +1,379 @@
+"""Benchmark of the batched convergent Born series solve on B200.
+
+Workload (one "step"): the batching configuration -- 128x128x64 grid at 50 nm, water background
+(eps_bg = 1.33^2), a seeded phantom of 12 non-overlapping beads (radius U[4,12] px, index U[1.36,1.60]),
+64 right-hand sides (32 illumination angles in an NA 1.2 cone snapped to the lattice x 2 polarisations),
+500 nm, periodic x,y and absorbing z (padded grid 128^3), tolerance 1e-6, GMRES as the reference runs it
+(no restart, maxiters = max(2*Bornmax, 100), warm start b); complex64 fields in HBM, FFT / Green /
+potential arithmetic in FP64 registers, classical Gram-Schmidt with FP64 dots (``--precision float32``
+runs the arithmetic in FP32 too).
+
+value : solves/s of that step with the potential resident in HBM and the fields left in HBM
+        (device time from CUDA events on the library's stream, max over ranks, weak scaling).
+e2e   : solves/s through the public API (fmcuda.solve_batch) from host permittivity to host E, H.
+Also reported: the plain FP64 GPU method (same algorithm with Krylov.jl's MGS, one RHS) and the
+relative L2 distance of the batched FP32 fields to it, the roofline of the dominant kernel class from
+live CUDA-event timing, and the CPU oracle baseline (numpy/scipy FP64, all host cores, bounded sample).
+
+`--impl reference` times the CPU restatement of the reference path (the reference is Julia, which this
+image does not have) on the same workload and prints its own line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+import warnings
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "frequencymaxwell.jl_b200"))
+
+GRID = (128, 128, 64)
+RES = (50e-9, 50e-9, 50e-9)
+WL = 500e-9
+EPS_BG = 1.33 ** 2
+SEED = 20261203
+NA = 1.2
+METRIC = "solves/s at rel-L2<=1e-5 vs FP64: batched FP32 vs plain FP64; p50/p99 latency"
+
+
+def batching_sources(n_angles=32, seed=SEED):
+    """32 (kx, ky) uniform in the NA 1.2 disk (sin(theta) <= NA/n_bg), snapped to the lattice
+    2*pi*m/(N*dx); polarisations s and p (two unit vectors orthogonal to k)."""
+    rng = np.random.default_rng(seed + 1)
+    nbg = math.sqrt(EPS_BG)
+    kbg = 2 * math.pi * nbg / WL
+    out = []
+    dk = [2 * math.pi / (GRID[d] * RES[d]) for d in range(2)]
+    while len(out) < n_angles:
+        r = math.sqrt(rng.uniform()) * NA / nbg
+        phi = rng.uniform(0, 2 * math.pi)
+        kx, ky = kbg * r * math.cos(phi), kbg * r * math.sin(phi)
+        kx = round(kx / dk[0]) * dk[0]
+        ky = round(ky / dk[1]) * dk[1]
+        st = math.hypot(kx, ky) / kbg
+        if st > NA / nbg:
+            continue
+        kz = math.sqrt(max(0.0, 1 - st * st))
+        k = np.array([kx / kbg, ky / kbg, kz])
+        k /= np.linalg.norm(k)
+        out.append(k)
+    pols = []
+    for k in out:
+        s = np.cross(k, [0.0, 0.0, 1.0])
+        if np.linalg.norm(s) < 1e-12:
+            s = np.array([0.0, 1.0, 0.0])
+        s /= np.linalg.norm(s)
+        p = np.cross(s, k)
+        p /= np.linalg.norm(p)
+        pols.append((k, s))
+        pols.append((k, p))
+    return pols
+
+
+def make_inputs():
+    import fmcuda as F
+    med = F.phantom_random_beads(GRID, 12, (4, 12), (1.36, 1.60), EPS_BG, SEED)
+    bc_z = F.AbsorbingBoundaryCondition(thickness=GRID[2] * RES[2], attenuation_thickness=GRID[2] * RES[2],
+                                        sharpness=1.0, profile=F.TanhProfile)
+    bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
+    srcs = [F.PlaneWaveSource(wavelength=WL, polarization=p, k_vector=k) for k, p in batching_sources()]
+    return med, bcs, srcs
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.rows.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(steps=1):
+    """Oracle (numpy/scipy FP64, all host cores) on a bounded sample of the workload: one RHS, the
+    set-up and right-hand side, two operator applications and 8 Gram-Schmidt projections are timed,
+    then the 100-iteration GMRES solve is assembled from the measured pieces:
+      T = t_setup + t_curl + 101 * t_matvec + sum_{j=0}^{99} (j + 2) * t_mgs_pair."""
+    from oracle import cbs_oracle as O
+    import fmcuda as F
+    med, _, srcs = make_inputs()
+    t_pad = GRID[2] * RES[2]
+    cfg = O.SolverConfig(RES, GRID, (O.PeriodicBC(), O.PeriodicBC(), O.AbsorbingBC(t_pad, t_pad, 1.0)))
+    s = srcs[0]
+    src = O.PlaneWave(WL, s.polarization, s.k_vector)
+    t0 = time.perf_counter()
+    pot = O.build_potential(cfg, med.permittivity, EPS_BG, WL)
+    Ei, Hi = O.incident_field(src, cfg, EPS_BG)
+    S = pot.V[..., None] * Ei + (1j * pot.eps_imag) * Ei
+    b = O.green_conv(S, cfg, pot.k_square)
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(2):
+        w = O.cbs_preconditioner(O.cbs_operator(b, pot.V, cfg, pot.k_square), pot.V, pot.eps_imag)
+    t_mv = (time.perf_counter() - t0) / 2
+    t0 = time.perf_counter()
+    for _ in range(8):
+        h = O._dot(b, w)
+        w = w - h * b
+    t_mgs = (time.perf_counter() - t0) / 8
+    t0 = time.perf_counter()
+    O.magnetic_field(b, RES, WL)
+    t_curl = time.perf_counter() - t0
+    iters = max(2 * pot.Bornmax, 100)
+    T = t_setup + t_curl + (iters + 1) * t_mv + sum((j + 2) * t_mgs for j in range(iters))
+    sample = (f"1 RHS of the workload: set-up + RHS, 2 operator applications, 8 MGS projections, 1 curl timed "
+              f"({t_setup:.2f}s, {t_mv:.2f}s/op, {t_mgs:.3f}s/proj); {iters}-iteration GMRES solve assembled "
+              f"from them")
+    return {"value": 1.0 / T, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port", "sample": sample,
+            "seconds_per_solve": T}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline()
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "batching 128x128x64, 12 beads, 64 RHS (sample: 1 RHS per step)",
+                       "grid": list(GRID), "padded": [128, 128, 128], "rhs": 64, "solver": "gmres-100"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run(args):
+    import torch
+    import fmcuda as F
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+
+    med, bcs, srcs = make_inputs()
+    srcs = srcs[: args.nrhs]
+    lists = [[s] for s in srcs]
+    solver = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
+                                    precision=args.precision, linear_solver=F.KrylovJL_GMRES(ortho=args.ortho),
+                                    max_rhs=args.nrhs, device_index=dev)
+    plan = solver.plan()
+    info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
+    opts = solver.solve_options(int(info.bornmax))
+    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", dev))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def step():
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            _, _, infos, st = plan.solve_plane_waves(lists, EPS_BG, opts, keep_on_device=True)
+        return infos
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    times = []
+    plan.set_profiling(True)
+    launches0 = plan.launch_count()
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            barrier()
+            ev0.record(stream)
+            infos = step()
+            ev1.record(stream)
+            ev1.synchronize()
+            times.append(ev0.elapsed_time(ev1) / 1000.0)
+            barrier()
+    launches = plan.launch_count() - launches0
+    kstats = plan.kernel_stats()
+    plan.set_profiling(False)
+    t_step = max(times)
+    if dist:
+        t = torch.tensor([statistics.median(times)], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_med = float(t.item())
+    else:
+        t_med = statistics.median(times)
+    value = world * args.nrhs / t_med
+    iters = [i.iterations for i in infos]
+
+    # end to end through the public API (host permittivity in, host E/H out)
+    e2e_times = []
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for _ in range(max(1, args.e2e_steps)):
+            barrier()
+            t0 = time.perf_counter()
+            outs = F.solve_batch(solver, lists, med)
+            barrier()
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_t = statistics.median(e2e_times)
+    g = int(np.prod(GRID))
+    h2d = g * 16 + sum(GRID[d] + 2 * solver.padding()[d] for d in range(3)) * 8
+    d2h = 2 * args.nrhs * 3 * g * 16
+
+    # plain FP64 GPU method (reference algorithm: GMRES with MGS, one RHS) and accuracy vs it
+    fp64 = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
+                                  precision="float64", linear_solver=F.KrylovJL_GMRES(ortho="mgs"), max_rhs=1,
+                                  device_index=dev)
+    t64 = []
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for _ in range(args.fp64_steps):
+            barrier()
+            t0 = time.perf_counter()
+            ref = F.solve(fp64, srcs[0], med)
+            barrier()
+            t64.append(time.perf_counter() - t0)
+    fp64_sps = 1.0 / statistics.median(t64)
+    from oracle.cbs_oracle import rel_l2
+    err_e = rel_l2(outs[0].E, ref.E)
+    err_h = rel_l2(outs[0].H, ref.H)
+    fp64_iters = fp64.iteration_count
+    fp64.release()
+
+    # roofline of the dominant kernel class (live CUDA-event timing over the timed steps)
+    peak, peak_kind = load_peaks()
+    dom = max(kstats.items(), key=lambda kv: kv[1]["ms"])
+    dname, ds = dom
+    achieved = ds["bytes"] / (ds["ms"] / 1000.0) / 1e9 if ds["ms"] > 0 else 0.0
+    total_ms = sum(v["ms"] for v in kstats.values())
+    traffic = None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": dname, "peak_kind": peak_kind,
+            "share": ds["ms"] / total_ms if total_ms > 0 else None,
+            "bytes_per_launch": ds["bytes"] / max(1, ds["launches"]),
+            "ms_per_launch": ds["ms"] / max(1, ds["launches"])}
+    all_bytes = sum(v["bytes"] for v in kstats.values())
+    classes = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                   "GBps": round(v["bytes"] / (v["ms"] / 1000) / 1e9, 1) if v["ms"] > 0 else None}
+               for k, v in kstats.items() if v["launches"]}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cb = cpu_baseline()
+    clocks = clk.summary()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_med * 1000.0, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "config": {"workload": "batching: 128x128x64 (padded 128^3), 12 seeded beads, "
+                                       f"{args.nrhs} RHS (32 NA-1.2 angles x 2 pol), GMRES-{opts.maxiters}",
+                           "grid": list(GRID), "padded": list(solver.padded_size()), "rhs_per_gpu": args.nrhs,
+                           "precision": f"{args.precision}: complex64 fields in HBM, FP64 dots"
+                                        + (", FP64 FFT/Green/V arithmetic" if args.precision != "float32" else ""),
+                           "ortho": args.ortho, "parallelism": f"replicas{world}",
+                           "l2": "inputs larger than L2 (Krylov basis of 50 MB vectors)", "seed": SEED},
+                "latency_s": {"p50": statistics.median(times), "p99": float(np.percentile(times, 99)),
+                              "unit": "batched step"},
+                "iterations": {"min": min(iters), "max": max(iters)},
+                "fp64_plain": {"solves_per_s": fp64_sps, "iterations": fp64_iters,
+                               "rel_l2_E_fp32_vs_fp64": err_e, "rel_l2_H_fp32_vs_fp64": err_h,
+                               "ratio_fp32_batched_over_fp64": value / world / fp64_sps},
+                "e2e": {"value": world * args.nrhs / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "roofline": roof, "kernel_classes": classes,
+                "algorithmic_GBps_all_kernels": all_bytes / (total_ms / 1000) / 1e9 if total_ms else None,
+                "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
+        print(json.dumps(line))
+    solver.release()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fmcuda", choices=["fmcuda", "reference"])
+    ap.add_argument("--nrhs", type=int, default=64)
+    ap.add_argument("--ortho", default="cgs", choices=["mgs", "cgs", "cgs2"])
+    ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

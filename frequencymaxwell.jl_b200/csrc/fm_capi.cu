@@ -68,11 +68,13 @@ bool is_pow2_in(int n, int lo, int hi) { return n >= lo && n <= hi && (n & (n - 
 struct fm_plan {
   fm_plan_desc desc{};
   int prec = FM_PREC_F32;
-  size_t esz = 8;  // bytes per complex element
+  size_t esz = 8;  // bytes per complex element in HBM
+  bool c64 = false;  // FFT / Green / V arithmetic in FP64 (FP64 storage, or FP32 storage with FP64 math)
   Dims dims{};
   PadInfo pi{};
   long long n = 0, M = 0;  // voxels, elements per field (3n)
   cudaStream_t st = nullptr;
+  int sms = 148;
   bool avg = false;     // any absorbing axis
   bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
   double shift[3] = {0, 0, 0};
@@ -90,7 +92,113 @@ struct fm_plan {
   DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
   DevBuf Eo, Ho;
   int out_nrhs = 0;
+  // launch accounting (always) and event timing per kernel class (when prof is on)
+  bool prof = false;
+  long long launches[16] = {0};
+  double kms[16] = {0}, kbytes[16] = {0};
+  long long total_launches = 0;
+  struct Pending { int cls; double bytes; cudaEvent_t a, b; };
+  std::vector<Pending> pend;
+  std::vector<cudaEvent_t> evpool;
 };
+
+// ---------------------------------------------------------------------------
+// kernel accounting
+// ---------------------------------------------------------------------------
+enum KCls { KC_XF = 0, KC_YF, KC_ZG, KC_YI, KC_XI, KC_DOT, KC_UPD, KC_MGS, KC_AXPBY, KC_CURL, KC_SETUP, KC_N };
+static const char* kcls_name[KC_N] = {"xf", "yf", "zg", "yi", "xi", "multidot", "update", "mgs", "axpby", "curl", "setup"};
+
+static cudaEvent_t ev_get(fm_plan* P) {
+  if (!P->evpool.empty()) {
+    cudaEvent_t e = P->evpool.back();
+    P->evpool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+static void tk_resolve(fm_plan* P) {
+  for (auto& q : P->pend) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, q.a, q.b) == cudaSuccess) {
+      P->kms[q.cls] += ms;
+      P->kbytes[q.cls] += q.bytes;
+    }
+    P->evpool.push_back(q.a);
+    P->evpool.push_back(q.b);
+  }
+  P->pend.clear();
+}
+
+struct Tk {
+  fm_plan* P;
+  int cls;
+  double bytes;
+  cudaEvent_t a;
+};
+static Tk tk_begin(fm_plan* P, int cls, double bytes) {
+  Tk t{P, cls, bytes, nullptr};
+  if (P->prof) {
+    if (P->pend.size() > 8192) {  // bound the number of outstanding events
+      cudaStreamSynchronize(P->st);
+      tk_resolve(P);
+    }
+    t.a = ev_get(P);
+    cudaEventRecord(t.a, P->st);
+  }
+  return t;
+}
+static void tk_end(const Tk& t) {
+  t.P->launches[t.cls]++;
+  t.P->total_launches++;
+  if (t.P->prof) {
+    cudaEvent_t b = ev_get(t.P);
+    cudaEventRecord(b, t.P->st);
+    t.P->pend.push_back({t.cls, t.bytes, t.a, b});
+  }
+}
+#define FM_TRACK(P, cls, bytes, stmt)          \
+  do {                                         \
+    Tk tk_ = tk_begin((P), (cls), (bytes));    \
+    stmt;                                      \
+    tk_end(tk_);                               \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// pass dispatch: storage type S, arithmetic double when the plan asks for it
+// ---------------------------------------------------------------------------
+template <typename S>
+static cudaError_t pass_xf(const fm_plan* P, const Dims& d, int pro, const void* in, const void* V, const double* rs,
+                           const void* tw, const void* ramp, void* out, const int* act) {
+  if constexpr (std::is_same<S, double>::value) return launch_xf<double, double>(d, pro, in, V, rs, tw, ramp, out, act, P->st);
+  else return P->c64 ? launch_xf<float, double>(d, pro, in, V, rs, tw, ramp, out, act, P->st)
+                     : launch_xf<float, float>(d, pro, in, V, rs, tw, ramp, out, act, P->st);
+}
+template <typename S>
+static cudaError_t pass_y(const fm_plan* P, const Dims& d, int dir, const void* in, const void* tw, const void* ramp,
+                          void* out, const int* act) {
+  if constexpr (std::is_same<S, double>::value) return launch_y<double, double>(d, dir, in, tw, ramp, out, act, P->st);
+  else return P->c64 ? launch_y<float, double>(d, dir, in, tw, ramp, out, act, P->st)
+                     : launch_y<float, float>(d, dir, in, tw, ramp, out, act, P->st);
+}
+template <typename S>
+static cudaError_t pass_zg(const fm_plan* P, const Dims& d, int mode, const void* in, const GreenParams& gp,
+                           const void* tw, const void* rz, void* out, const int* act) {
+  if constexpr (std::is_same<S, double>::value) return launch_zg<double, double>(d, mode, in, gp, tw, rz, out, act, P->st);
+  else return P->c64 ? launch_zg<float, double>(d, mode, in, gp, tw, rz, out, act, P->st)
+                     : launch_zg<float, float>(d, mode, in, gp, tw, rz, out, act, P->st);
+}
+template <typename S>
+static cudaError_t pass_xi(const fm_plan* P, const Dims& d, int epi, const void* in, const void* V, const void* xv,
+                           const void* bv, const double* rs, const EpiParams& ep, const void* tw, const void* ramp,
+                           void* out, const int* act) {
+  if constexpr (std::is_same<S, double>::value)
+    return launch_xi<double, double>(d, epi, in, V, xv, bv, rs, ep, tw, ramp, out, act, P->st);
+  else return P->c64 ? launch_xi<float, double>(d, epi, in, V, xv, bv, rs, ep, tw, ramp, out, act, P->st)
+                     : launch_xi<float, float>(d, epi, in, V, xv, bv, rs, ep, tw, ramp, out, act, P->st);
+}
 
 // ---------------------------------------------------------------------------
 // tables
@@ -148,16 +256,27 @@ static fm_status init_tables(fm_plan* P) {
 // ---------------------------------------------------------------------------
 // workspace
 // ---------------------------------------------------------------------------
-static int red_blocks(const fm_plan* P, int nb) {
-  int sms = 148;
-  int per = std::max(1, (4 * sms + nb - 1) / nb);
-  long long chunk = (long long)KV_THREADS * KV_EPT;
-  long long maxb = (P->M + chunk - 1) / chunk;
-  return (int)std::max(1LL, std::min<long long>(per, maxb));
+// Blocks per RHS for a Krylov kernel: one full wave of resident blocks
+// (SMs x occupancy) shared by the nb right-hand sides, so no launch ends with a
+// partly filled second wave.
+template <typename Kern>
+static int kv_blocks(const fm_plan* P, Kern kern, int nb) {
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, KV_THREADS, 0) != cudaSuccess || bps < 1) bps = 1;
+  const long long cap = (long long)P->sms * bps;
+  const long long chunk = (long long)KV_THREADS * KV_EPT;
+  const long long maxb = (P->M + chunk - 1) / chunk;
+  return (int)std::max(1LL, std::min<long long>(maxb, cap / nb));
+}
+static int red_blocks_max(const fm_plan* P, int nb) {
+  // upper bound of kv_blocks over all kernels (at most 8 blocks of 256 threads per SM)
+  const long long chunk = (long long)KV_THREADS * KV_EPT;
+  const long long maxb = (P->M + chunk - 1) / chunk;
+  return (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * 8 / nb));
 }
 
 static fm_status ensure_reduce(fm_plan* P, int nb, int K) {
-  const int nblk = red_blocks(P, nb);
+  const int nblk = red_blocks_max(P, nb);
   FM_CK(P->red_part.ensure((size_t)nb * nblk * (KV_KMAX + 2) * sizeof(double2)));
   FM_CK(P->red_out.ensure((size_t)nb * (KV_KMAX + 2) * sizeof(double2)));
   if (P->red_cnt.cap < (size_t)nb * sizeof(unsigned)) {
@@ -177,8 +296,15 @@ static fm_status ensure_reduce(fm_plan* P, int nb, int K) {
 // ---------------------------------------------------------------------------
 template <typename R>
 static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
-                          const void* bv, const EpiParams& ep, void* out, const int* act) {
+                          const void* bv, const EpiParams& ep, void* out, const int* act, int nact = -1) {
   using T = cplx<R>;
+  if (nact < 0) nact = nb;
+  const double fbA = (double)nact * P->M * sizeof(T), vb = (double)nact * P->n * sizeof(T);
+  double xib = 2 * fbA;
+  if (epi != EPI_STORE) xib += fbA;
+  if (epi == EPI_PREC_RES) xib += fbA;
+  if (epi == EPI_PREC_OP || epi == EPI_PREC_RES) xib += vb;
+  if (epi == EPI_OP && (ep.beta_re != 0.0 || ep.beta_im != 0.0)) xib += fbA;
   Dims d = P->dims;
   d.nb = nb;
   const size_t fbytes = (size_t)nb * P->M * sizeof(T);
@@ -194,12 +320,20 @@ static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const dou
     const int mode = P->zonly ? ZMODE_AVG2 : ZMODE_ONE;
     gp.shift[2] = P->zonly ? P->shift[2] : 0.0;
     gp.scale_re = 1.0 / ((double)P->n * (P->zonly ? 2.0 : 1.0));
-    FM_CK(launch_xf<R>(d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act, P->st));
-    FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act, P->st));
-    FM_CK(launch_zg<R>(d, mode, P->t2.p, gp, P->zonly ? P->twz2.p : P->twz.p, P->zonly ? P->rz.p : nullptr, P->t1.p,
-                       act, P->st));
-    FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act, P->st));
-    FM_CK(launch_xi<R>(d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act, P->st));
+    cudaError_t e;
+    FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
+             e = pass_xf<R>(P, d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_YF, 2 * fbA, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_ZG, 2 * fbA,
+             e = pass_zg<R>(P, d, mode, P->t2.p, gp, P->zonly ? P->twz2.p : P->twz.p, P->zonly ? P->rz.p : nullptr,
+                              P->t1.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_YI, 2 * fbA, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_XI, xib, e = pass_xi<R>(P, d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act));
+    FM_CK(e);
     return FM_OK;
   }
   // general case (sub-pixel shifts on x or y): the two branches run separately and are averaged
@@ -211,23 +345,28 @@ static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const dou
 // ---------------------------------------------------------------------------
 template <typename R>
 static fm_status multidot(fm_plan* P, int nb, int K, const void* U, const void* w, bool wnorm, const int* act,
-                          std::vector<double2>& host_out) {
+                          std::vector<double2>& host_out, int nact = -1) {
   FM_TRY(ensure_reduce(P, nb, K));
-  const int nblk = red_blocks(P, nb);
+  if (nact < 0) nact = nb;
+  const int nblk = wnorm ? kv_blocks(P, k_multidot<R, true>, nb) : kv_blocks(P, k_multidot<R, false>, nb);
   dim3 g(nblk, nb);
+  const double bytes = (double)(K + 1) * nact * P->M * sizeof(cplx<R>);
   if (wnorm)
-    k_multidot<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
-                                                     (double2*)P->red_part.p, (double2*)P->red_out.p,
-                                                     (unsigned*)P->red_cnt.p, act);
+    FM_TRACK(P, KC_DOT, bytes,
+             (k_multidot<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
+                                                               (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                               (unsigned*)P->red_cnt.p, act)));
   else
-    k_multidot<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
-                                                      (double2*)P->red_part.p, (double2*)P->red_out.p,
-                                                      (unsigned*)P->red_cnt.p, act);
+    FM_TRACK(P, KC_DOT, bytes,
+             (k_multidot<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, (const cplx<R>*)U, (const cplx<R>*)w,
+                                                                (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                                (unsigned*)P->red_cnt.p, act)));
   FM_CK(cudaGetLastError());
   const int KK = K + (wnorm ? 1 : 0);
   host_out.resize((size_t)nb * KK);
   FM_CK(cudaMemcpyAsync(host_out.data(), P->red_out.p, host_out.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
   FM_CK(cudaStreamSynchronize(P->st));
+  tk_resolve(P);
   return FM_OK;
 }
 
@@ -246,21 +385,25 @@ static fm_status axpby3(fm_plan* P, int nb, const void* a, const std::vector<cd>
   }
   FM_CK(cudaMemcpyAsync(P->coef.p, h.data(), h.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
   const double2* cp = (const double2*)P->coef.p;
-  const int nblk = red_blocks(P, nb);
+  const int nblk = norm ? kv_blocks(P, k_axpby3<R, true>, nb) : kv_blocks(P, k_axpby3<R, false>, nb);
   dim3 g(nblk, nb);
   using T = cplx<R>;
+  const double bytes = (double)((a ? 1 : 0) + (b ? 1 : 0) + (c ? 1 : 0) + 1) * nb * P->M * sizeof(T);
   if (norm)
-    k_axpby3<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c, cp + 2 * nb,
-                                                   (T*)y, (double2*)P->red_part.p, (double2*)P->red_out.p,
-                                                   (unsigned*)P->red_cnt.p, act);
+    FM_TRACK(P, KC_AXPBY, bytes,
+             (k_axpby3<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c,
+                                                             cp + 2 * nb, (T*)y, (double2*)P->red_part.p,
+                                                             (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
   else
-    k_axpby3<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c,
-                                                    cp + 2 * nb, (T*)y, nullptr, nullptr, nullptr, act);
+    FM_TRACK(P, KC_AXPBY, bytes,
+             (k_axpby3<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, (const T*)a, cp, (const T*)b, cp + nb, (const T*)c,
+                                                              cp + 2 * nb, (T*)y, nullptr, nullptr, nullptr, act)));
   FM_CK(cudaGetLastError());
   if (norm) {
     std::vector<double2> o(nb);
     FM_CK(cudaMemcpyAsync(o.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     FM_CK(cudaStreamSynchronize(P->st));
+    tk_resolve(P);
     nrm->resize(nb);
     for (int i = 0; i < nb; ++i) (*nrm)[i] = o[i].x;
   }
@@ -380,29 +523,34 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
       // w = M^{-1} A v_j  into U[j+1]
       T* Uj = U + (size_t)j * nb * fe;
       T* Uw = U + (size_t)(j + 1) * nb * fe;
-      FM_TRY(green_op<R>(P, nb, Uj, PRO_V_SCALE, sc + (size_t)j * nb, EPI_PREC_OP, Uj, nullptr, ep, Uw, act));
+      int nact = 0;
+      for (int b = 0; b < nb; ++b) nact += acth[b];
+      const double fbA = (double)nact * fe * sizeof(T);
+      FM_TRY(green_op<R>(P, nb, Uj, PRO_V_SCALE, sc + (size_t)j * nb, EPI_PREC_OP, Uj, nullptr, ep, Uw, act, nact));
       // orthogonalise against v_0..v_j
       const int K = j + 1;
       std::vector<double2> hcol((size_t)nb * (K + 1));
-      const int nblk = red_blocks(P, nb);
-      dim3 g(nblk, nb);
       if (o.ortho == FM_ORTHO_MGS) {
         double2* hd = (double2*)P->hbuf.p;
         const int hs = KV_KMAX + 2;
+        dim3 g(kv_blocks(P, k_mgs<R>, nb), nb);
         for (int i = 0; i <= K; ++i) {
-          k_mgs<R><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, i, K, U, sc, nb, Uw, hd, hs, (double2*)P->red_part.p,
-                                                (unsigned*)P->red_cnt.p, act);
+          const double mb = fbA * ((i > 0 ? 1 : 0) + (i < K ? 1 : 0) + 1 + (i > 0 ? 1 : 0));
+          FM_TRACK(P, KC_MGS, mb,
+                   (k_mgs<R><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, i, K, U, sc, nb, Uw, hd, hs,
+                                                          (double2*)P->red_part.p, (unsigned*)P->red_cnt.p, act)));
         }
         FM_CK(cudaGetLastError());
         std::vector<double2> hh((size_t)nb * hs);
         FM_CK(cudaMemcpyAsync(hh.data(), hd, hh.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
         FM_CK(cudaStreamSynchronize(P->st));
+        tk_resolve(P);
         for (int b = 0; b < nb; ++b)
           for (int i = 0; i <= K; ++i) hcol[(size_t)b * (K + 1) + i] = hh[(size_t)b * hs + i];
       } else {
         // classical Gram-Schmidt (optionally twice), FP64 coefficients
         std::vector<double2> hr;
-        FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr));
+        FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr, nact));
         std::vector<double2> htot((size_t)nb * K);
         for (int b = 0; b < nb; ++b)
           for (int i = 0; i < K; ++i) {
@@ -416,15 +564,20 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
           FM_CK(P->coef.ensure((size_t)nb * K * sizeof(double2)));
           FM_CK(cudaMemcpyAsync(P->coef.p, hr.data(), hr.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
           Coef cf{(const double2*)P->coef.p, K, sc, nb, -1.0, 0};
+          const double ub = (K + 2) * fbA;
+          dim3 g(last ? kv_blocks(P, k_update<R, true>, nb) : kv_blocks(P, k_update<R, false>, nb), nb);
           if (last)
-            k_update<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr, (double2*)P->red_part.p,
-                                                           (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act);
+            FM_TRACK(P, KC_UPD, ub,
+                     (k_update<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr,
+                                                                     (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                                     (unsigned*)P->red_cnt.p, act)));
           else
-            k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr, nullptr, nullptr, nullptr,
-                                                            act);
+            FM_TRACK(P, KC_UPD, ub,
+                     (k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, cf, Uw, nullptr, nullptr, nullptr,
+                                                                      nullptr, act)));
           FM_CK(cudaGetLastError());
           if (!last) {
-            FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr));
+            FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr, nact));
             for (int b = 0; b < nb; ++b)
               for (int i = 0; i < K; ++i) {
                 double s = sch[(size_t)i * nb + b];
@@ -436,6 +589,7 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
         std::vector<double2> nn(nb);
         FM_CK(cudaMemcpyAsync(nn.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
         FM_CK(cudaStreamSynchronize(P->st));
+        tk_resolve(P);
         for (int b = 0; b < nb; ++b) {
           for (int i = 0; i < K; ++i) hcol[(size_t)b * (K + 1) + i] = htot[(size_t)b * K + i];
           hcol[(size_t)b * (K + 1) + K] = nn[b];
@@ -516,9 +670,10 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
       FM_CK(cudaMemcpyAsync(P->coef.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
       FM_CK(cudaMemcpyAsync(sc, sch.data(), (size_t)(KV_KMAX + 1) * nb * sizeof(double), cudaMemcpyHostToDevice, P->st));
       Coef cf{(const double2*)P->coef.p, KV_KMAX + 1, sc, nb, 1.0, 1};
-      dim3 g(red_blocks(P, nb), nb);
-      k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, Kmax, U, cf, (T*)P->xbuf.p, nullptr, nullptr, nullptr,
-                                                      nullptr, nullptr);
+      dim3 g(kv_blocks(P, k_update<R, false>, nb), nb);
+      FM_TRACK(P, KC_UPD, (double)(Kmax + 2) * nb * fe * sizeof(T),
+               (k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, Kmax, U, cf, (T*)P->xbuf.p, nullptr, nullptr,
+                                                                nullptr, nullptr, nullptr)));
       FM_CK(cudaGetLastError());
     }
     any = false;
@@ -727,12 +882,20 @@ static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
   const double f = P->wavelength / (2.0 * M_PI * 377.0) / (double)P->n;
   gp.scale_re = 0.0;
   gp.scale_im = -f;
-  FM_CK(launch_xf<R>(d, PRO_COPY, P->xbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr, P->st));
-  FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
-  FM_CK(launch_zg<R>(d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr, P->st));
-  FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
-  FM_CK(launch_xi<R>(d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
-                     nullptr, P->st));
+  const double cb = 2.0 * nb * P->M * sizeof(T);
+  cudaError_t e;
+  FM_TRACK(P, KC_CURL, cb, e = pass_xf<R>(P, d, PRO_COPY, P->xbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr));
+  FM_CK(e);
+  FM_TRACK(P, KC_CURL, cb, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
+  FM_CK(e);
+  FM_TRACK(P, KC_CURL, cb, e = pass_zg<R>(P, d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr));
+  FM_CK(e);
+  FM_TRACK(P, KC_CURL, cb, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
+  FM_CK(e);
+  FM_TRACK(P, KC_CURL, cb,
+           e = pass_xi<R>(P, d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr,
+                            P->ebuf.p, nullptr));
+  FM_CK(e);
   return FM_OK;
 }
 
@@ -796,6 +959,9 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   const size_t avail = (size_t)((freeb + held) * 0.92);
   wave = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, avail / per));
   wave = std::min(wave, std::max(1, P->desc.max_rhs));
+  // balance the waves: ceil(nrhs / waves) right-hand sides each
+  const int waves = (nrhs + wave - 1) / wave;
+  wave = (nrhs + waves - 1) / waves;
   if ((size_t)wave * per > avail) return fail(FM_ERR_OOM, "one right-hand side does not fit in device memory");
   return FM_OK;
 }
@@ -829,8 +995,8 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
     if (desc->pad[a] < 0) return fail(FM_ERR_INVALID, "padding must be >= 0");
     if (!(desc->resolution[a] > 0)) return fail(FM_ERR_INVALID, "all resolution components must be positive");
   }
-  if (desc->precision != FM_PREC_F32 && desc->precision != FM_PREC_F64)
-    return fail(FM_ERR_INVALID, "precision must be FM_PREC_F32 or FM_PREC_F64");
+  if (desc->precision != FM_PREC_F32 && desc->precision != FM_PREC_F64 && desc->precision != FM_PREC_F32_MATH64)
+    return fail(FM_ERR_INVALID, "precision must be FM_PREC_F32, FM_PREC_F64 or FM_PREC_F32_MATH64");
   int nd = 0;
   if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) return fail(FM_ERR_CUDA, "no CUDA device");
   if (desc->device < 0 || desc->device >= nd) return fail(FM_ERR_INVALID, "device ordinal out of range");
@@ -843,16 +1009,18 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   if (avg && !zonly) return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build");
   if (zonly && n3[2] > AXIS_MAX_AVG2)
     return fail(FM_ERR_UNSUPPORTED, "padded z size above 256 with an absorbing z boundary is not supported by this build");
-  const int prec = desc->precision;
-  const int pwy = prec == FM_PREC_F64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
-  const int pwz = prec == FM_PREC_F64 ? pencils_per_warp<double>(zonly ? 2 * n3[2] : n3[2])
-                                      : pencils_per_warp<float>(zonly ? 2 * n3[2] : n3[2]);
+  const int prec = desc->precision == FM_PREC_F64 ? FM_PREC_F64 : FM_PREC_F32;  // storage
+  const bool c64 = desc->precision != FM_PREC_F32;                                   // arithmetic
+  const int pwy = c64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
+  const int pwz = c64 ? pencils_per_warp<double>(zonly ? 2 * n3[2] : n3[2])
+                      : pencils_per_warp<float>(zonly ? 2 * n3[2] : n3[2]);
   if (pwy <= 0 || pwz <= 0 || n3[0] % pwy || n3[0] % pwz) return fail(FM_ERR_UNSUPPORTED, "x size too small for pencil tiling");
   if (cudaSetDevice(desc->device) != cudaSuccess) return fail(FM_ERR_CUDA, "cudaSetDevice failed");
   fm_plan* P = new fm_plan();
   P->desc = *desc;
   if (P->desc.max_rhs < 1) P->desc.max_rhs = 1;
   P->prec = prec;
+  P->c64 = c64;
   P->esz = prec == FM_PREC_F64 ? 16 : 8;
   P->dims = Dims{n3[0], n3[1], n3[2], 1, (long long)n3[0] * n3[1] * n3[2]};
   P->n = P->dims.n;
@@ -861,11 +1029,15 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   P->avg = avg;
   P->zonly = zonly;
   for (int a = 0; a < 3; ++a) P->shift[a] = desc->absorbing[a] ? 0.25 : 0.0;
+  {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, desc->device) == cudaSuccess) P->sms = prop.multiProcessorCount;
+  }
   if (cudaStreamCreateWithFlags(&P->st, cudaStreamNonBlocking) != cudaSuccess) {
     delete P;
     return fail(FM_ERR_CUDA, "stream creation failed");
   }
-  fm_status s = prec == FM_PREC_F64 ? init_tables<double>(P) : init_tables<float>(P);
+  fm_status s = c64 ? init_tables<double>(P) : init_tables<float>(P);
   if (s != FM_OK) {
     fm_plan_destroy(P);
     return s;
@@ -884,6 +1056,8 @@ void fm_plan_destroy(fm_plan* P) {
                     &P->hbuf, &P->eps_dev, &P->fx, &P->fy, &P->fz, &P->maxpart, &P->maxout, &P->wt_x,
                     &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho};
   for (DevBuf* b : bufs) b->release();
+  tk_resolve(P);
+  for (cudaEvent_t e : P->evpool) cudaEventDestroy(e);
   if (P->st) cudaStreamDestroy(P->st);
   delete P;
 }
@@ -944,12 +1118,12 @@ static fm_status apply_host(fm_plan* P, int nrhs, const double* x, double* y, in
     for (int a = 0; a < 3; ++a)
       gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]);
     gp.scale_im = -P->wavelength / (2.0 * M_PI * 377.0) / (double)P->n;
-    FM_CK(launch_xf<R>(d, PRO_COPY, P->sbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr, P->st));
-    FM_CK(launch_y<R>(d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
-    FM_CK(launch_zg<R>(d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr, P->st));
-    FM_CK(launch_y<R>(d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr, P->st));
-    FM_CK(launch_xi<R>(d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
-                       nullptr, P->st));
+    FM_CK(pass_xf<R>(P, d, PRO_COPY, P->sbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr));
+    FM_CK(pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
+    FM_CK(pass_zg<R>(P, d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr));
+    FM_CK(pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
+    FM_CK(pass_xi<R>(P, d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
+                       nullptr));
   }
   FM_TRY(d2h_field<R>(P, P->ebuf.p, cnt, 1.0, y));
   return FM_OK;
@@ -1203,21 +1377,24 @@ static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_
     FM_CK(P->sbuf.ensure((size_t)nb * P->M * sizeof(cplx<R>)));
     WaveTabs wt{(const double2*)P->wt_x.p, (const double2*)P->wt_y.p, (const double2*)P->wt_z.p,
                 (const double2*)P->wt_pe.p, (const double2*)P->wt_ph.p, (const int*)P->wt_first.p};
-    k_source_term<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->V.p, P->eps_imag / P->kref2,
-                                                       (cplx<R>*)P->sbuf.p, nullptr);
+    FM_TRACK(P, KC_SETUP, (double)nb * P->M * sizeof(cplx<R>) + (double)P->n * sizeof(cplx<R>),
+             (k_source_term<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->V.p,
+                                                                 P->eps_imag / P->kref2, (cplx<R>*)P->sbuf.p, nullptr)));
     FM_CK(cudaGetLastError());
     std::vector<fm_solve_info> inf(nb);
     FM_TRY(solve_core<R>(P, nb, o, inf));
     double2* eo = (double2*)P->Eo.p + (keep ? (size_t)b0 * 3 * g : 0);
     double2* ho = (double2*)P->Ho.p + (keep ? (size_t)b0 * 3 * g : 0);
-    k_assemble<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->xbuf.p,
-                                                    (const cplx<R>*)P->ebuf.p, eo, ho);
+    FM_TRACK(P, KC_SETUP, (double)nb * 3 * g * (2 * sizeof(cplx<R>) + 2 * sizeof(double2)),
+             (k_assemble<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->xbuf.p,
+                                                              (const cplx<R>*)P->ebuf.p, eo, ho)));
     FM_CK(cudaGetLastError());
     if (!keep) {
       FM_CK(cudaMemcpyAsync(E + (size_t)b0 * 3 * g * 2, eo, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
       FM_CK(cudaMemcpyAsync(H + (size_t)b0 * 3 * g * 2, ho, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     }
     FM_CK(cudaStreamSynchronize(P->st));
+    tk_resolve(P);
     for (int b = 0; b < nb; ++b) {
       if (info) info[b0 + b] = inf[b];
       all_ok &= inf[b].solved != 0;
@@ -1260,3 +1437,37 @@ fm_status fm_copy_fields(fm_plan* P, int nrhs, double* E, double* H) {
   return FM_OK;
 }
 
+
+fm_status fm_set_profiling(fm_plan* P, int on) {
+  if (!P) return fail(FM_ERR_INVALID, "null plan");
+  FM_CK(cudaSetDevice(P->desc.device));
+  FM_CK(cudaStreamSynchronize(P->st));
+  tk_resolve(P);
+  P->prof = on != 0;
+  for (int i = 0; i < KC_N; ++i) {
+    P->launches[i] = 0;
+    P->kms[i] = 0;
+    P->kbytes[i] = 0;
+  }
+  P->total_launches = 0;
+  return FM_OK;
+}
+
+int fm_kernel_stats(fm_plan* P, fm_kernel_stat* out, int max) {
+  if (!P) return -1;
+  cudaSetDevice(P->desc.device);
+  cudaStreamSynchronize(P->st);
+  tk_resolve(P);
+  int n = 0;
+  for (int i = 0; i < KC_N && n < max; ++i, ++n) {
+    std::snprintf(out[n].name, sizeof(out[n].name), "%s", kcls_name[i]);
+    out[n].launches = P->launches[i];
+    out[n].ms = P->kms[i];
+    out[n].bytes = P->kbytes[i];
+  }
+  return n;
+}
+
+long long fm_launch_count(fm_plan* P) { return P ? P->total_launches : -1; }
+
+void* fm_stream(fm_plan* P) { return P ? (void*)P->st : nullptr; }

@@ -1,5 +1,6 @@
-// Host-side launchers of the axis passes (implemented per precision in
-// fm_pass_f32.cu / fm_pass_f64.cu so the two instantiation sets compile in parallel).
+// Host-side launchers of the axis passes.  S is the storage type of the fields in
+// HBM, R the arithmetic type in registers (S = R, or float storage with double
+// arithmetic).  Each (S, R) pair is instantiated in its own translation unit.
 #pragma once
 #include <cuda_runtime.h>
 #include "fm_passes.cuh"
@@ -11,16 +12,16 @@ namespace fm {
 constexpr int AXIS_MAX = 512;
 constexpr int AXIS_MAX_AVG2 = 256;
 
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, const double* rhs_scale, const void* twx,
                       const void* rampx, void* out, const int* active, cudaStream_t st);
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_y(const Dims& d, int dir, const void* in, const void* twy, const void* rampy, void* out,
                      const int* active, cudaStream_t st);
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_zg(const Dims& d, int mode, const void* in, const GreenParams& gp, const void* twz, const void* rz,
                       void* out, const int* active, cudaStream_t st);
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
                       const double* rhs_scale, const EpiParams& ep, const void* twx, const void* rampx, void* out,
                       const int* active, cudaStream_t st);

@@ -1,14 +1,15 @@
-// Axis-pass launchers instantiated for float.
+// Axis-pass launchers instantiated for storage float, arithmetic float.
 #include "fm_pass_impl.cuh"
 
 namespace fm {
-template cudaError_t launch_xf<float>(const Dims&, int, const void*, const void*, const double*, const void*, const void*,
-                                      void*, const int*, cudaStream_t);
-template cudaError_t launch_y<float>(const Dims&, int, const void*, const void*, const void*, void*, const int*,
+template cudaError_t launch_xf<float, float>(const Dims&, int, const void*, const void*, const double*, const void*,
+                                      const void*, void*, const int*, cudaStream_t);
+template cudaError_t launch_y<float, float>(const Dims&, int, const void*, const void*, const void*, void*, const int*,
                                      cudaStream_t);
-template cudaError_t launch_zg<float>(const Dims&, int, const void*, const GreenParams&, const void*, const void*, void*,
-                                      const int*, cudaStream_t);
-template cudaError_t launch_xi<float>(const Dims&, int, const void*, const void*, const void*, const void*, const double*,
-                                      const EpiParams&, const void*, const void*, void*, const int*, cudaStream_t);
+template cudaError_t launch_zg<float, float>(const Dims&, int, const void*, const GreenParams&, const void*, const void*,
+                                      void*, const int*, cudaStream_t);
+template cudaError_t launch_xi<float, float>(const Dims&, int, const void*, const void*, const void*, const void*,
+                                      const double*, const EpiParams&, const void*, const void*, void*, const int*,
+                                      cudaStream_t);
 template int pencils_per_warp<float>(int);
 }  // namespace fm

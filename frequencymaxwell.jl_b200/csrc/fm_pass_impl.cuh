@@ -12,65 +12,70 @@ static void allow_smem(K kern, size_t bytes) {
 constexpr int ROW_THREADS = 256;
 constexpr int ZG_THREADS = 128;
 
-template <typename R, int L, int PRO>
+template <typename S, typename R, int L, int PRO>
 static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const double* rs, const void* tw, const void* ramp,
                         void* out, const int* act, cudaStream_t st) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
-  allow_smem(k_xf<R, L, PRO>, smem);
-  k_xf<R, L, PRO><<<blocks, ROW_THREADS, smem, st>>>(d, (const T*)in, (const T*)V, rs, (const T*)tw, (const T*)ramp,
-                                                      (T*)out, act);
+  allow_smem(k_xf<S, R, L, PRO>, smem);
+  k_xf<S, R, L, PRO><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, rs, (const T*)tw,
+                                                         (const T*)ramp, (TS*)out, act);
   return cudaGetLastError();
 }
 
-template <typename R, int L, int EPI>
+template <typename S, typename R, int L, int EPI>
 static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void* xv, const void* bv, const double* rs,
                         const EpiParams& ep, const void* tw, const void* ramp, void* out, const int* act,
                         cudaStream_t st) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
-  allow_smem(k_xi<R, L, EPI>, smem);
-  k_xi<R, L, EPI><<<blocks, ROW_THREADS, smem, st>>>(d, (const T*)in, (const T*)V, (const T*)xv, (const T*)bv, rs, ep,
-                                                      (const T*)tw, (const T*)ramp, (T*)out, act);
+  allow_smem(k_xi<S, R, L, EPI>, smem);
+  k_xi<S, R, L, EPI><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, (const TS*)bv,
+                                                         rs, ep, (const T*)tw, (const T*)ramp, (TS*)out, act);
   return cudaGetLastError();
 }
 
-template <typename R, int L, int DIR>
+template <typename S, typename R, int L, int DIR>
 static cudaError_t y_L(const Dims& d, const void* in, const void* tw, const void* ramp, void* out, const int* act,
                        cudaStream_t st) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
   const long long warps = (long long)(d.nx / PW) * d.nz * 3 * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
-  allow_smem(k_y<R, L, DIR>, smem);
-  k_y<R, L, DIR><<<blocks, ROW_THREADS, smem, st>>>(d, (const T*)in, (const T*)tw, (const T*)ramp, (T*)out, act);
+  allow_smem(k_y<S, R, L, DIR>, smem);
+  k_y<S, R, L, DIR><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const T*)tw, (const T*)ramp, (TS*)out, act);
   return cudaGetLastError();
 }
 
-template <typename R, int L, int MODE>
+template <typename S, typename R, int L, int MODE>
 static cudaError_t zg_L(const Dims& d, const void* in, const GreenParams& gp, const void* tw, const void* rz, void* out,
                         const int* act, cudaStream_t st) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   constexpr int LF = (MODE == ZMODE_AVG2) ? 2 * L : L;
   using P_ = Plan<LF, R>;
   constexpr int PW = 32 / P_::TP, W = ZG_THREADS / 32;
   const long long warps = (long long)(d.nx / PW) * d.ny * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(LF + L + W * PW * SmemLen<LF>::v) * sizeof(T);
-  allow_smem(k_zg<R, L, MODE>, smem);
-  k_zg<R, L, MODE><<<blocks, ZG_THREADS, smem, st>>>(d, (const T*)in, gp, (const T*)tw, (const T*)rz, (T*)out, act);
+  allow_smem(k_zg<S, R, L, MODE>, smem);
+  k_zg<S, R, L, MODE><<<blocks, ZG_THREADS, smem, st>>>(d, (const TS*)in, gp, (const T*)tw, (const T*)rz, (TS*)out,
+                                                         act);
   return cudaGetLastError();
 }
 
@@ -86,10 +91,10 @@ static cudaError_t zg_L(const Dims& d, const void* in, const GreenParams& gp, co
     default: return cudaErrorInvalidValue;          \
   }
 
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, const double* rs, const void* tw,
                       const void* ramp, void* out, const int* act, cudaStream_t st) {
-#define XF_(LL, P) xf_L<R, LL, P>(d, in, V, rs, tw, ramp, out, act, st)
+#define XF_(LL, P) xf_L<S, R, LL, P>(d, in, V, rs, tw, ramp, out, act, st)
 #define XF0(LL) XF_(LL, PRO_COPY)
 #define XF1(LL) XF_(LL, PRO_V)
 #define XF2(LL) XF_(LL, PRO_V_SCALE)
@@ -102,11 +107,11 @@ cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, con
 #undef XF2
 }
 
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
                       const double* rs, const EpiParams& ep, const void* tw, const void* ramp, void* out,
                       const int* act, cudaStream_t st) {
-#define XI_(LL, E) xi_L<R, LL, E>(d, in, V, xv, bv, rs, ep, tw, ramp, out, act, st)
+#define XI_(LL, E) xi_L<S, R, LL, E>(d, in, V, xv, bv, rs, ep, tw, ramp, out, act, st)
 #define XI0(LL) XI_(LL, EPI_STORE)
 #define XI1(LL) XI_(LL, EPI_OP)
 #define XI2(LL) XI_(LL, EPI_PREC_OP)
@@ -122,23 +127,23 @@ cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, con
 #undef XI3
 }
 
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_y(const Dims& d, int dir, const void* in, const void* tw, const void* ramp, void* out,
                      const int* act, cudaStream_t st) {
-#define YF(LL) y_L<R, LL, -1>(d, in, tw, ramp, out, act, st)
-#define YI(LL) y_L<R, LL, +1>(d, in, tw, ramp, out, act, st)
+#define YF(LL) y_L<S, R, LL, -1>(d, in, tw, ramp, out, act, st)
+#define YI(LL) y_L<S, R, LL, +1>(d, in, tw, ramp, out, act, st)
   if (dir < 0) { FM_SWITCH_L(d.ny, YF, YF) }
   FM_SWITCH_L(d.ny, YI, YI)
 #undef YF
 #undef YI
 }
 
-template <typename R>
+template <typename S, typename R>
 cudaError_t launch_zg(const Dims& d, int mode, const void* in, const GreenParams& gp, const void* tw, const void* rz,
                       void* out, const int* act, cudaStream_t st) {
-#define ZA(LL) zg_L<R, LL, ZMODE_AVG2>(d, in, gp, tw, rz, out, act, st)
-#define ZO(LL) zg_L<R, LL, ZMODE_ONE>(d, in, gp, tw, rz, out, act, st)
-#define ZC(LL) zg_L<R, LL, ZMODE_CURL>(d, in, gp, tw, rz, out, act, st)
+#define ZA(LL) zg_L<S, R, LL, ZMODE_AVG2>(d, in, gp, tw, rz, out, act, st)
+#define ZO(LL) zg_L<S, R, LL, ZMODE_ONE>(d, in, gp, tw, rz, out, act, st)
+#define ZC(LL) zg_L<S, R, LL, ZMODE_CURL>(d, in, gp, tw, rz, out, act, st)
   if (mode == ZMODE_AVG2) {
     switch (d.nz) {
       case 8: return ZA(8);

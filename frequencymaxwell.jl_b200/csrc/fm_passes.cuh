@@ -17,6 +17,13 @@
 
 namespace fm {
 
+// storage <-> compute conversion (identity when the types match)
+template <typename To, typename From>
+__device__ __forceinline__ To cv(From a) {
+  if constexpr (std::is_same<To, From>::value) return a;
+  else return mk((typename RealOf<To>::R)a.x, (typename RealOf<To>::R)a.y);
+}
+
 struct Dims {
   int nx, ny, nz, nb;
   long long n;  // nx*ny*nz
@@ -40,12 +47,13 @@ __device__ __forceinline__ void load_table(T* dst, const T* src, int n) {
 // ---------------------------------------------------------------------------
 enum { PRO_COPY = 0, PRO_V = 1, PRO_V_SCALE = 2 };
 
-template <typename R, int L, int PRO>
-__global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ V,
+template <typename S, typename R, int L, int PRO>
+__global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
                                             const double* __restrict__ rhs_scale, const cplx<R>* __restrict__ twx,
-                                            const cplx<R>* __restrict__ rampx, cplx<R>* __restrict__ out,
+                                            const cplx<R>* __restrict__ rampx, cplx<S>* __restrict__ out,
                                             const int* __restrict__ active) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -65,7 +73,7 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ 
   T vrow[E];
   if constexpr (PRO != PRO_COPY) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) vrow[e] = V[yz * L + lay_idx<L, E, P_::R0>(t, e)];
+    for (int e = 0; e < E; ++e) vrow[e] = cv<T>(V[yz * L + lay_idx<L, E, P_::R0>(t, e)]);
   }
   R s = R(1);
   if constexpr (PRO == PRO_V_SCALE) s = (R)rhs_scale[b];
@@ -76,7 +84,7 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ 
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int x = lay_idx<L, E, P_::R0>(t, e);
-      T a = in[base + x];
+      T a = cv<T>(in[base + x]);
       if constexpr (PRO != PRO_COPY) a = cmul(a, vrow[e]);
       if constexpr (PRO == PRO_V_SCALE) a = cscale(a, s);
       if (rampx) a = cmul(a, rampx[x]);
@@ -84,7 +92,7 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ 
     }
     fft_fwd_plan<-1, P_>(v, sm, tw, t);
 #pragma unroll
-    for (int e = 0; e < E; ++e) out[base + lay_idx<L, E, P_::RL>(t, e)] = v[e];
+    for (int e = 0; e < E; ++e) out[base + lay_idx<L, E, P_::RL>(t, e)] = cv<TS>(v[e]);
     __syncwarp();
   }
 }
@@ -94,11 +102,12 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<R>* __restrict__ 
 // x columns at fixed (z, c, b); lane = t*P + p so consecutive lanes read
 // consecutive x.
 // ---------------------------------------------------------------------------
-template <typename R, int L, int DIR>
-__global__ void __launch_bounds__(256) k_y(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ twy,
-                                           const cplx<R>* __restrict__ rampy, cplx<R>* __restrict__ out,
+template <typename S, typename R, int L, int DIR>
+__global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ in, const cplx<R>* __restrict__ twy,
+                                           const cplx<R>* __restrict__ rampy, cplx<S>* __restrict__ out,
                                            const int* __restrict__ active) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -123,23 +132,23 @@ __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<R>* __restrict__ i
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int y = lay_idx<L, E, P_::R0>(t, e);
-      T a = in[base + (long long)y * d.nx];
+      T a = cv<T>(in[base + (long long)y * d.nx]);
       if (rampy) a = cmul(a, rampy[y]);
       v[e] = a;
     }
     fft_fwd_plan<-1, P_>(v, sm, tw, t);
 #pragma unroll
-    for (int e = 0; e < E; ++e) out[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx] = v[e];
+    for (int e = 0; e < E; ++e) out[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx] = cv<TS>(v[e]);
   } else {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = in[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx];
+    for (int e = 0; e < E; ++e) v[e] = cv<T>(in[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx]);
     fft_rev_plan<+1, P_>(v, sm, tw, t);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int y = lay_idx<L, E, P_::R0>(t, e);
       T a = v[e];
       if (rampy) a = cmul(a, cconj(rampy[y]));
-      out[base + (long long)y * d.nx] = a;
+      out[base + (long long)y * d.nx] = cv<TS>(a);
     }
   }
 }
@@ -176,11 +185,12 @@ __device__ __forceinline__ R kidx_curl(int i, int n) {
   return (R)(i < (n >> 1) ? i : i - n);
 }
 
-template <typename R, int L, int MODE>
-__global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<R>* __restrict__ in, GreenParams gp,
+template <typename S, typename R, int L, int MODE>
+__global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ in, GreenParams gp,
                                             const cplx<R>* __restrict__ twz, const cplx<R>* __restrict__ rz,
-                                            cplx<R>* __restrict__ out, const int* __restrict__ active) {
+                                            cplx<S>* __restrict__ out, const int* __restrict__ active) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   constexpr int LF = (MODE == ZMODE_AVG2) ? 2 * L : L;
   using P_ = Plan<LF, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
@@ -214,7 +224,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<R>* __restrict__ 
       const int z = lay_idx<LF, E, P_::R0>(t, e);
       T a = czero<T>();
       if (MODE != ZMODE_AVG2 || z < L) {
-        a = in[base0 + (long long)c * d.n + (long long)z * plane];
+        a = cv<T>(in[base0 + (long long)c * d.n + (long long)z * plane]);
         if (MODE != ZMODE_CURL && rz) a = cmul(a, rtab[z]);
       }
       v[c][e] = a;
@@ -285,7 +295,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<R>* __restrict__ 
       if (MODE != ZMODE_AVG2 || z < L) {
         T a = v[c][e];
         if (MODE != ZMODE_CURL && rz) a = cmul(a, cconj(rtab[z]));
-        out[base0 + (long long)c * d.n + (long long)z * plane] = a;
+        out[base0 + (long long)c * d.n + (long long)z * plane] = cv<TS>(a);
       }
     }
   }
@@ -306,13 +316,14 @@ struct EpiParams {
   double inv_eps;  // 1/eps_imag (scaled units)
 };
 
-template <typename R, int L, int EPI>
-__global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<R>* __restrict__ in, const cplx<R>* __restrict__ V,
-                                            const cplx<R>* __restrict__ xv, const cplx<R>* __restrict__ bv,
+template <typename S, typename R, int L, int EPI>
+__global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
+                                            const cplx<S>* __restrict__ xv, const cplx<S>* __restrict__ bv,
                                             const double* __restrict__ rhs_scale, EpiParams ep,
                                             const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ rampx,
-                                            cplx<R>* __restrict__ out, const int* __restrict__ active) {
+                                            cplx<S>* __restrict__ out, const int* __restrict__ active) {
   using T = cplx<R>;
+  using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -334,7 +345,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<R>* __restrict__ 
     const R ie = (R)ep.inv_eps;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      T vv = V[yz * L + lay_idx<L, E, P_::R0>(t, e)];
+      T vv = cv<T>(V[yz * L + lay_idx<L, E, P_::R0>(t, e)]);
       gam[e] = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
     }
   }
@@ -346,7 +357,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<R>* __restrict__ 
     const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
     T v[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = in[base + lay_idx<L, E, P_::RL>(t, e)];
+    for (int e = 0; e < E; ++e) v[e] = cv<T>(in[base + lay_idx<L, E, P_::RL>(t, e)]);
     fft_rev_plan<+1, P_>(v, sm, tw, t);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -358,18 +369,18 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<R>* __restrict__ 
       if constexpr (EPI == EPI_STORE) {
         r = g;
       } else if constexpr (EPI == EPI_OP) {
-        T xx = xv[ix];
+        T xx = cv<T>(xv[ix]);
         T a = cmul(al, csub(xx, g));
-        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, out[ix]));
+        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(out[ix])));
         r = a;
       } else if constexpr (EPI == EPI_PREC_OP) {
-        T xx = cscale(xv[ix], s);
+        T xx = cscale(cv<T>(xv[ix]), s);
         r = cmul(gam[e], csub(xx, g));
       } else {
-        T xx = cscale(xv[ix], s);
-        r = cmul(gam[e], cadd(csub(bv[ix], xx), g));
+        T xx = cscale(cv<T>(xv[ix]), s);
+        r = cmul(gam[e], cadd(csub(cv<T>(bv[ix]), xx), g));
       }
-      out[ix] = r;
+      out[ix] = cv<TS>(r);
     }
     __syncwarp();
   }

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libfmcuda.so")
 
 FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_NOT_CONVERGED, FM_ERR_NONFINITE, FM_ERR_TIMEOUT, FM_ERR_CUDA, \
     FM_ERR_UNSUPPORTED = range(8)
-FM_PREC_F64, FM_PREC_F32 = 0, 1
+FM_PREC_F64, FM_PREC_F32, FM_PREC_F32_MATH64 = 0, 1, 2
 FM_METHOD_GMRES, FM_METHOD_BICGSTAB, FM_METHOD_RICHARDSON = 0, 1, 2
 FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2 = 0, 1, 2
 
@@ -30,6 +30,7 @@ EXPORTED = (
     "fm_abi_version", "fm_last_error", "fm_device_count", "fm_plan_create", "fm_plan_destroy", "fm_plan_bytes",
     "fm_set_potential", "fm_green_apply", "fm_apply_operator", "fm_apply_preconditioner", "fm_curl_field",
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
+    "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream",
 )
 
 
@@ -55,6 +56,10 @@ class fm_potential_info(C.Structure):
 class fm_plane_wave(C.Structure):
     _fields_ = [("wavelength", C.c_double), ("polarization", C.c_double * 6), ("k_vector", C.c_double * 3),
                 ("amplitude", C.c_double), ("phase", C.c_double)]
+
+
+class fm_kernel_stat(C.Structure):
+    _fields_ = [("name", C.c_char * 16), ("launches", C.c_longlong), ("ms", C.c_double), ("bytes", C.c_double)]
 
 
 class FMError(RuntimeError):
@@ -96,9 +101,16 @@ def lib() -> C.CDLL:
                                        C.POINTER(fm_solve_opts), P, P, C.POINTER(fm_solve_info)]
     L.fm_copy_fields.argtypes = [P, C.c_int, P, P]
     L.fm_synchronize.argtypes = [P]
+    L.fm_set_profiling.argtypes = [P, C.c_int]
+    L.fm_kernel_stats.argtypes = [P, C.POINTER(fm_kernel_stat), C.c_int]
+    L.fm_kernel_stats.restype = C.c_int
+    L.fm_launch_count.argtypes = [P]
+    L.fm_launch_count.restype = C.c_longlong
+    L.fm_stream.argtypes = [P]
+    L.fm_stream.restype = C.c_void_p
     for name in ("fm_plan_create", "fm_set_potential", "fm_green_apply", "fm_apply_operator",
                  "fm_apply_preconditioner", "fm_curl_field", "fm_solve_source", "fm_build_potential",
-                 "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize"):
+                 "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize", "fm_set_profiling"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L

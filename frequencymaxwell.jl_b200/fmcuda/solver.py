@@ -32,7 +32,7 @@ from .sources import PlaneWaveSource, as_list, source_wavelength
 class KrylovJL_GMRES:
     """GMRES as LinearSolve's KrylovJL_GMRES runs it (default: no restart).  ``gmres_restart`` > 0
     gives GMRES(m).  ``ortho`` picks the Gram-Schmidt variant ("mgs" as Krylov.jl, "cgs", "cgs2");
-    None chooses MGS for FP64 and CGS2 for FP32."""
+    None chooses MGS for FP64 (Krylov.jl's choice) and classical Gram-Schmidt for the FP32 forms."""
     gmres_restart: int = 0
     ortho: Optional[str] = None
 
@@ -59,7 +59,8 @@ class ConvergentBornSolver:
     tolerance=1e-6, linear_solver=KrylovJL_GMRES(), preconditioner="none", device="fmcuda")
     (convergent_born.jl:87-233).
 
-    ``precision`` ("float64" / "float32") replaces Julia's element-type parameter T; by default it is
+    ``precision`` ("float64" / "float32" / "float32-math64": FP32 fields in HBM with FP64 arithmetic in the
+    FFT, Green and potential kernels) replaces Julia's element-type parameter T; by default it is
     float32 when ``resolution`` holds numpy float32 values and float64 otherwise (the reference promotes
     the type of resolution and tolerance).  ``max_rhs`` bounds the batch held on the device at once."""
 
@@ -69,8 +70,8 @@ class ConvergentBornSolver:
                  max_rhs: int = 64, device_index: int = 0):
         if precision is None:
             precision = "float32" if all(isinstance(r, np.float32) for r in resolution) else "float64"
-        if precision not in ("float32", "float64"):
-            raise ValueError("precision must be 'float32' or 'float64'")
+        if precision not in ("float32", "float64", "float32-math64"):
+            raise ValueError("precision must be 'float32', 'float64' or 'float32-math64'")
         if device not in ("fmcuda", "cuda"):
             raise ValueError(f"GPU backend :{device} is not available. This package runs on the fmcuda "
                              f"(CUDA, sm_100a) backend only; it has no CPU path.")
@@ -143,7 +144,7 @@ class ConvergentBornSolver:
         ls = self.linear_solver
         if isinstance(ls, KrylovJL_GMRES):
             o.method = L.FM_METHOD_GMRES
-            ortho = ls.ortho or ("mgs" if self.precision == "float64" else "cgs2")
+            ortho = ls.ortho or ("mgs" if self.precision == "float64" else "cgs")
             o.ortho = _ORTHO[ortho]
             o.restart = int(ls.gmres_restart)
         elif isinstance(ls, KrylovJL_BICGSTAB):
@@ -196,7 +197,8 @@ class DevicePlan:
             d.pad[a] = int(pad[a])
             d.resolution[a] = float(resolution[a])
             d.absorbing[a] = int(bool(absorbing[a]))
-        d.precision = L.FM_PREC_F64 if precision == "float64" else L.FM_PREC_F32
+        d.precision = {"float64": L.FM_PREC_F64, "float32": L.FM_PREC_F32,
+                       "float32-math64": L.FM_PREC_F32_MATH64}[precision]
         d.max_rhs = int(max_rhs)
         d.device = int(device)
         self.desc = d
@@ -312,6 +314,25 @@ class DevicePlan:
                                           info)
         L.check(st, allow_not_converged=True)
         return E, H, list(info), st
+
+    # -- instrumentation --
+    def set_profiling(self, on: bool):
+        L.check(L.lib().fm_set_profiling(self.handle, int(bool(on))))
+
+    def kernel_stats(self):
+        arr = (L.fm_kernel_stat * 16)()
+        n = L.lib().fm_kernel_stats(self.handle, arr, 16)
+        return {arr[i].name.decode(): dict(launches=arr[i].launches, ms=arr[i].ms, bytes=arr[i].bytes)
+                for i in range(max(n, 0))}
+
+    def launch_count(self) -> int:
+        return int(L.lib().fm_launch_count(self.handle))
+
+    def stream(self) -> int:
+        return int(L.lib().fm_stream(self.handle) or 0)
+
+    def synchronize(self):
+        L.check(L.lib().fm_synchronize(self.handle))
 
     def copy_fields(self, n: int):
         shp = self.grid + (3, n)

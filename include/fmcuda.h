@@ -39,7 +39,9 @@ typedef enum {
   FM_ERR_UNSUPPORTED = 7   /* size or option this build does not support */
 } fm_status;
 
-enum { FM_PREC_F64 = 0, FM_PREC_F32 = 1 };
+/* FM_PREC_F32_MATH64: fields stored as complex FP32 in HBM (FP32 traffic), FFT / Green / potential
+ * arithmetic carried out in FP64 registers. */
+enum { FM_PREC_F64 = 0, FM_PREC_F32 = 1, FM_PREC_F32_MATH64 = 2 };
 enum { FM_METHOD_GMRES = 0, FM_METHOD_BICGSTAB = 1, FM_METHOD_RICHARDSON = 2 };
 enum { FM_ORTHO_MGS = 0, FM_ORTHO_CGS = 1, FM_ORTHO_CGS2 = 2 };
 
@@ -54,7 +56,7 @@ typedef struct {
   int pad[3];           /* padding pixels per side and axis */
   double resolution[3]; /* voxel size in metres */
   int absorbing[3];     /* 1: absorbing axis -> shift 0.25 and (G(+s)+G(-s))/2 averaging */
-  int precision;        /* FM_PREC_F64 or FM_PREC_F32 */
+  int precision;        /* FM_PREC_F64, FM_PREC_F32 or FM_PREC_F32_MATH64 */
   int max_rhs;          /* largest batch the plan will be asked to hold at once (>= 1) */
   int device;           /* CUDA device ordinal */
 } fm_plan_desc;
@@ -156,6 +158,24 @@ fm_status fm_copy_fields(fm_plan* plan, int nrhs, double* E_out, double* H_out);
 
 /* Wait for the plan's stream. */
 fm_status fm_synchronize(fm_plan* plan);
+
+/* ---- instrumentation (no reference counterpart: measurement support) ---- */
+
+typedef struct {
+  char name[16];        /* kernel class: xf, yf, zg, yi, xi, multidot, update, mgs, axpby, curl, setup */
+  long long launches;   /* launches since the last fm_set_profiling */
+  double ms;            /* summed device time from CUDA events on the plan stream (profiling on) */
+  double bytes;         /* summed algorithmic HBM bytes of those launches */
+} fm_kernel_stat;
+
+/* Reset the counters; on != 0 also brackets every launch with CUDA events on the plan's stream. */
+fm_status fm_set_profiling(fm_plan* plan, int on);
+/* Fill up to max entries (one per kernel class); returns the number written. */
+int fm_kernel_stats(fm_plan* plan, fm_kernel_stat* out, int max);
+/* Kernel launches issued by the plan since the last fm_set_profiling. */
+long long fm_launch_count(fm_plan* plan);
+/* The plan's cudaStream_t, for callers that time work on it with their own events. */
+void* fm_stream(fm_plan* plan);
 
 #ifdef __cplusplus
 }
