@@ -105,12 +105,19 @@ __device__ __forceinline__ void bfly(T* v) {
   else static_assert(RAD == 2, "unsupported radix");
 }
 
-// ---- shared-memory exchange: one padding slot every 16 elements (bank spread) ----
-__device__ __forceinline__ int sm_phys(int i) { return i + (i >> 4); }
-template <int L> struct SmemLen { static constexpr int v = L + L / 16; };
+// ---- shared-memory exchange: one padding slot every 128 bytes of data ----
+// (every 16 elements of float2, every 8 of double2), so the strided stage writes
+// of consecutive lanes fall in distinct banks.
+template <typename T>
+__device__ __forceinline__ int sm_phys(int i) {
+  return sizeof(T) == 16 ? i + (i >> 3) : i + (i >> 4);
+}
 
 // One Stockham stage: radix RAD, NS = product of the radices already applied.
-// tw is a table of exp(-2*pi*i*k/L), k in [0, L).
+// tw is the stage-twiddle table of the radix order being run: for the stage with
+// prior product NS, entry (NS - 1) + (q - 1)*NS + k holds exp(-2*pi*i*k*q/(NS*RAD)),
+// k in [0, NS), q in [1, RAD).  Consecutive lanes (consecutive k) read consecutive
+// entries, and the stages together need exactly L - 1 entries.
 template <int DIR, int L, int E, int RAD, int NS, bool LAST, typename T>
 __device__ __forceinline__ void fft_stage(T (&v)[E], T* sm, const T* tw, int t) {
   constexpr int TP = L / E;
@@ -123,7 +130,7 @@ __device__ __forceinline__ void fft_stage(T (&v)[E], T* sm, const T* tw, int t) 
     if constexpr (NS > 1) {
 #pragma unroll
       for (int q = 1; q < RAD; ++q) {
-        T w = tw[k * q * (L / (NS * RAD))];
+        T w = tw[(NS - 1) + (q - 1) * NS + k];
         if constexpr (DIR > 0) w = cconj(w);
         v[m * RAD + q] = cmul(v[m * RAD + q], w);
       }
@@ -132,7 +139,7 @@ __device__ __forceinline__ void fft_stage(T (&v)[E], T* sm, const T* tw, int t) 
     if constexpr (!LAST) {
       const int base = (j / NS) * NS * RAD + k;
 #pragma unroll
-      for (int q = 0; q < RAD; ++q) sm[sm_phys(base + q * NS)] = v[m * RAD + q];
+      for (int q = 0; q < RAD; ++q) sm[sm_phys<T>(base + q * NS)] = v[m * RAD + q];
     }
   }
 }
@@ -143,7 +150,7 @@ __device__ __forceinline__ void fft_gather(T (&v)[E], const T* sm, int t) {
 #pragma unroll
   for (int m = 0; m < E / RAD; ++m)
 #pragma unroll
-    for (int q = 0; q < RAD; ++q) v[m * RAD + q] = sm[sm_phys(t + TP * m + q * (L / RAD))];
+    for (int q = 0; q < RAD; ++q) v[m * RAD + q] = sm[sm_phys<T>(t + TP * m + q * (L / RAD))];
 }
 
 // Full FFT of one pencil with the radix sequence (R0, R1, R2) (zeros = unused).
@@ -197,17 +204,33 @@ FM_PLAN(256, double, 8, 8, 8, 4)
 FM_PLAN(512, double, 16, 16, 8, 4)
 #undef FM_PLAN
 
+// forward-order run (radices R0, R1, R2) with its stage-twiddle table
 template <int DIR, typename P, typename T>
-__device__ __forceinline__ void fft_fwd_plan(T (&v)[P::E], T* sm, const T* tw, int t) {
-  fft_run<DIR, P::L, P::E, P::R0, P::R1, P::R2>(v, sm, tw, t);
+__device__ __forceinline__ void fft_fwd_plan(T (&v)[P::E], T* sm, const T* tw_fwd, int t) {
+  fft_run<DIR, P::L, P::E, P::R0, P::R1, P::R2>(v, sm, tw_fwd, t);
 }
-// inverse-direction run with the radices reversed (consumes the RL-layout, returns the R0-layout)
+// reversed-order run (consumes the RL-layout, returns the R0-layout) with its own table
 template <int DIR, typename P, typename T>
-__device__ __forceinline__ void fft_rev_plan(T (&v)[P::E], T* sm, const T* tw, int t) {
-  if constexpr (P::R1 == 0) fft_run<DIR, P::L, P::E, P::R0, 0, 0>(v, sm, tw, t);
-  else if constexpr (P::R2 == 0) fft_run<DIR, P::L, P::E, P::R1, P::R0, 0>(v, sm, tw, t);
-  else fft_run<DIR, P::L, P::E, P::R2, P::R1, P::R0>(v, sm, tw, t);
+__device__ __forceinline__ void fft_rev_plan(T (&v)[P::E], T* sm, const T* tw_rev, int t) {
+  if constexpr (P::R1 == 0) fft_run<DIR, P::L, P::E, P::R0, 0, 0>(v, sm, tw_rev, t);
+  else if constexpr (P::R2 == 0) fft_run<DIR, P::L, P::E, P::R1, P::R0, 0>(v, sm, tw_rev, t);
+  else fft_run<DIR, P::L, P::E, P::R2, P::R1, P::R0>(v, sm, tw_rev, t);
 }
+
+// Padded pencil stride in the exchange buffer.  A shared-memory wavefront serves
+// 128 bytes: 16 lanes of 8-byte or 8 lanes of 16-byte elements.  With lanes
+// t-fastest (x rows) a wavefront spans 128/size/TP pencils, each using TP
+// consecutive bank slots; with lanes pencil-fastest (y, z) it spans PW pencils
+// with 128/size/PW slots each.  The stride is the padded length rounded up to
+// the residue (mod 128 bytes) that puts those pencils on disjoint banks.
+template <int L, typename T, int TP, bool TFAST>
+struct PencilStride {
+  static constexpr int units = 128 / (int)sizeof(T);
+  static constexpr int base = sizeof(T) == 16 ? L + L / 8 : L + L / 16;
+  static constexpr int PW = 32 / TP;
+  static constexpr int r = TFAST ? (TP % units) : (PW >= units ? 0 : (units / PW) % units);
+  static constexpr int v = base + ((r - base % units) % units + units) % units;
+};
 
 // index held in register e = m*R + q under the R-layout
 template <int L, int E, int R>

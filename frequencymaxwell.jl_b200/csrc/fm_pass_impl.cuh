@@ -22,7 +22,7 @@ static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const doub
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
-  const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
+  const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xf<S, R, L, PRO>, smem);
   k_xf<S, R, L, PRO><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, rs, (const T*)tw,
                                                          (const T*)ramp, (TS*)out, act);
@@ -40,7 +40,7 @@ static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
-  const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
+  const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xi<S, R, L, EPI>, smem);
   k_xi<S, R, L, EPI><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, (const TS*)bv,
                                                          rs, ep, (const T*)tw, (const T*)ramp, (TS*)out, act);
@@ -56,7 +56,7 @@ static cudaError_t y_L(const Dims& d, const void* in, const void* tw, const void
   constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
   const long long warps = (long long)(d.nx / PW) * d.nz * 3 * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
-  const size_t smem = (size_t)(L + W * PW * SmemLen<L>::v) * sizeof(T);
+  const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, false>::v) * sizeof(T);
   allow_smem(k_y<S, R, L, DIR>, smem);
   k_y<S, R, L, DIR><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const T*)tw, (const T*)ramp, (TS*)out, act);
   return cudaGetLastError();
@@ -72,7 +72,7 @@ static cudaError_t zg_L(const Dims& d, const void* in, const GreenParams& gp, co
   constexpr int PW = 32 / P_::TP, W = ZG_THREADS / 32;
   const long long warps = (long long)(d.nx / PW) * d.ny * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
-  const size_t smem = (size_t)(LF + L + W * PW * SmemLen<LF>::v) * sizeof(T);
+  const size_t smem = (size_t)(2 * LF + L + W * PW * PencilStride<LF, T, P_::TP, false>::v) * sizeof(T);
   allow_smem(k_zg<S, R, L, MODE>, smem);
   k_zg<S, R, L, MODE><<<blocks, ZG_THREADS, smem, st>>>(d, (const TS*)in, gp, (const T*)tw, (const T*)rz, (TS*)out,
                                                          act);

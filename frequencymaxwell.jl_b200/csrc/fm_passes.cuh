@@ -29,11 +29,14 @@ struct Dims {
   long long n;  // nx*ny*nz
 };
 
-// Warp-local exchange buffers: each warp owns P pencils x SmemLen<L>.
-template <typename T, int LFFT>
+// Warp-local exchange buffers: each warp owns PW pencils of STRIDE elements.
+template <typename T, int STRIDE>
 __device__ __forceinline__ T* warp_smem(T* base, int warp_in_cta, int pencils_per_warp, int p) {
-  return base + ((size_t)warp_in_cta * pencils_per_warp + p) * SmemLen<LFFT>::v;
+  return base + ((size_t)warp_in_cta * pencils_per_warp + p) * STRIDE;
 }
+
+// Twiddle tables per FFT length are stored as [forward-order stage table (L) |
+// reversed-order stage table (L)] (see fft_stage).
 
 template <typename T>
 __device__ __forceinline__ void load_table(T* dst, const T* src, int n) {
@@ -69,7 +72,7 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<S>* __restrict__ 
   const int b = (int)(row / ((long long)d.ny * d.nz));
   if (active && !active[b]) return;
   const long long yz = row - (long long)b * d.ny * d.nz;
-  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T* sm = warp_smem<T, PencilStride<L, T, TP, true>::v>(ex, wic, PW, p);
   T vrow[E];
   if constexpr (PRO != PRO_COPY) {
 #pragma unroll
@@ -113,7 +116,7 @@ __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ i
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tw = reinterpret_cast<T*>(smraw);
   T* ex = tw + L;
-  load_table(tw, twy, L);
+  load_table(tw, twy + (DIR < 0 ? 0 : L), L);
   __syncthreads();
   const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
   const int p = lane % PW, t = lane / PW;
@@ -126,7 +129,7 @@ __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ i
   const int b = (int)(zcb / (3LL * d.nz));
   if (active && !active[b]) return;
   const long long base = zcb * (long long)d.ny * d.nx + x;
-  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T* sm = warp_smem<T, PencilStride<L, T, TP, false>::v>(ex, wic, PW, p);
   T v[E];
   if constexpr (DIR < 0) {
 #pragma unroll
@@ -196,9 +199,10 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tw = reinterpret_cast<T*>(smraw);
-  T* rtab = tw + LF;
+  T* twr = tw + LF;
+  T* rtab = twr + LF;
   T* ex = rtab + L;
-  load_table(tw, twz, LF);
+  load_table(tw, twz, 2 * LF);
   if (rz) load_table(rtab, rz, L);
   __syncthreads();
   const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
@@ -214,7 +218,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
   if (active && !active[b]) return;
   const long long plane = (long long)d.nx * d.ny;
   const long long base0 = (long long)b * 3 * d.n + (long long)y * d.nx + x;
-  T* sm = warp_smem<T, LF>(ex, wic, PW, p);
+  T* sm = warp_smem<T, PencilStride<LF, T, TP, false>::v>(ex, wic, PW, p);
 
   T v[3][E];
 #pragma unroll
@@ -287,7 +291,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
 
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    fft_rev_plan<+1, P_>(v[c], sm, tw, t);
+    fft_rev_plan<+1, P_>(v[c], sm, twr, t);
     __syncwarp();
 #pragma unroll
     for (int e = 0; e < E; ++e) {
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tw = reinterpret_cast<T*>(smraw);
   T* ex = tw + L;
-  load_table(tw, twx, L);
+  load_table(tw, twx + L, L);
   __syncthreads();
   const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
   const int p = lane / TP, t = lane % TP;
@@ -339,7 +343,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
   const int b = (int)(row / ((long long)d.ny * d.nz));
   if (active && !active[b]) return;
   const long long yz = row - (long long)b * d.ny * d.nz;
-  T* sm = warp_smem<T, L>(ex, wic, PW, p);
+  T* sm = warp_smem<T, PencilStride<L, T, TP, true>::v>(ex, wic, PW, p);
   T gam[E];
   if constexpr (EPI == EPI_PREC_OP || EPI == EPI_PREC_RES) {
     const R ie = (R)ep.inv_eps;
