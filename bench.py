@@ -358,6 +358,27 @@ def run(args):
     return 0
 
 
+def run_operator_case(args):
+    """Small case for profilers: `reps` applications of the CBS operator on `nrhs` seeded random fields
+    on the bench grid (no solve)."""
+    import fmcuda as F
+    med, bcs, _ = make_inputs()
+    rng = np.random.default_rng(0)
+    shp = (128, 128, 128, 3, args.nrhs)
+    x = np.asfortranarray(rng.standard_normal(shp) + 1j * rng.standard_normal(shp))
+    s = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, precision=args.precision,
+                               max_rhs=args.nrhs)
+    p = s.plan()
+    p.build_potential(med.permittivity, EPS_BG, WL, s.attenuation_filters(), -1)
+    t0 = time.perf_counter()
+    for _ in range(args.reps):
+        y = p.apply_operator(x)
+    print(json.dumps({"operator_case": args.precision, "nrhs": args.nrhs, "reps": args.reps,
+                      "s_per_rep_host": (time.perf_counter() - t0) / args.reps, "mean_abs": float(np.abs(y).mean())}))
+    s.release()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,7 +391,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--operator-case", action="store_true", help="profiling case: operator applications only")
+    ap.add_argument("--reps", type=int, default=3)
     args = ap.parse_args()
+    if args.operator_case:
+        return run_operator_case(args)
     if args.impl == "reference":
         return run_reference(args)
     return run(args)

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <complex>
@@ -75,6 +76,8 @@ struct fm_plan {
   long long n = 0, M = 0;  // voxels, elements per field (3n)
   cudaStream_t st = nullptr;
   int sms = 148;
+  bool use_tma = true;  // TMA-staged y/z passes (FMCUDA_NO_TMA=1 selects the register-only passes)
+  DevBuf errbuf;        // device error code written by bounded pipeline waits
   bool avg = false;     // any absorbing axis
   bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
   double shift[3] = {0, 0, 0};
@@ -179,6 +182,15 @@ static cudaError_t pass_xf(const fm_plan* P, const Dims& d, int pro, const void*
 template <typename S>
 static cudaError_t pass_y(const fm_plan* P, const Dims& d, int dir, const void* in, const void* tw, const void* ramp,
                           void* out, const int* act) {
+  if (P->use_tma && !ramp) {
+    cudaError_t e;
+    if constexpr (std::is_same<S, double>::value)
+      e = launch_y_tma<double, double>(d, dir, in, tw, ramp, out, act, (int*)P->errbuf.p, P->sms, P->st);
+    else
+      e = P->c64 ? launch_y_tma<float, double>(d, dir, in, tw, ramp, out, act, (int*)P->errbuf.p, P->sms, P->st)
+                 : launch_y_tma<float, float>(d, dir, in, tw, ramp, out, act, (int*)P->errbuf.p, P->sms, P->st);
+    if (e != cudaErrorNotSupported) return e;
+  }
   if constexpr (std::is_same<S, double>::value) return launch_y<double, double>(d, dir, in, tw, ramp, out, act, P->st);
   else return P->c64 ? launch_y<float, double>(d, dir, in, tw, ramp, out, act, P->st)
                      : launch_y<float, float>(d, dir, in, tw, ramp, out, act, P->st);
@@ -186,6 +198,15 @@ static cudaError_t pass_y(const fm_plan* P, const Dims& d, int dir, const void* 
 template <typename S>
 static cudaError_t pass_zg(const fm_plan* P, const Dims& d, int mode, const void* in, const GreenParams& gp,
                            const void* tw, const void* rz, void* out, const int* act) {
+  if (P->use_tma) {
+    cudaError_t e;
+    if constexpr (std::is_same<S, double>::value)
+      e = launch_zg_tma<double, double>(d, mode, in, gp, tw, rz, out, act, (int*)P->errbuf.p, P->sms, P->st);
+    else
+      e = P->c64 ? launch_zg_tma<float, double>(d, mode, in, gp, tw, rz, out, act, (int*)P->errbuf.p, P->sms, P->st)
+                 : launch_zg_tma<float, float>(d, mode, in, gp, tw, rz, out, act, (int*)P->errbuf.p, P->sms, P->st);
+    if (e != cudaErrorNotSupported) return e;
+  }
   if constexpr (std::is_same<S, double>::value) return launch_zg<double, double>(d, mode, in, gp, tw, rz, out, act, P->st);
   else return P->c64 ? launch_zg<float, double>(d, mode, in, gp, tw, rz, out, act, P->st)
                      : launch_zg<float, float>(d, mode, in, gp, tw, rz, out, act, P->st);
@@ -886,6 +907,18 @@ static fm_status richardson(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
   return FM_OK;
 }
 
+// reads (and clears) the device error code set by bounded pipeline waits
+static fm_status check_device_error(fm_plan* P) {
+  int code = 0;
+  FM_CK(cudaMemcpyAsync(&code, P->errbuf.p, sizeof(int), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  if (code) {
+    cudaMemsetAsync(P->errbuf.p, 0, sizeof(int), P->st);
+    return fail(FM_ERR_TIMEOUT, "a TMA pipeline wait timed out on the device (code " + std::to_string(code) + ")");
+  }
+  return FM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // shared solve core: from scaled source terms in P->sbuf (nb RHS) to the
 // scattered field in P->xbuf and its curl in P->ebuf.
@@ -933,7 +966,7 @@ static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
            e = pass_xi<R>(P, d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr,
                             P->ebuf.p, nullptr));
   FM_CK(e);
-  return FM_OK;
+  return check_device_error(P);
 }
 
 // ---------------------------------------------------------------------------
@@ -1074,6 +1107,14 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
     delete P;
     return fail(FM_ERR_CUDA, "stream creation failed");
   }
+  {
+    const char* no_tma = std::getenv("FMCUDA_NO_TMA");
+    P->use_tma = !(no_tma && no_tma[0] == '1');
+  }
+  if (P->errbuf.ensure(sizeof(int)) != cudaSuccess || cudaMemsetAsync(P->errbuf.p, 0, sizeof(int), P->st) != cudaSuccess) {
+    fm_plan_destroy(P);
+    return fail(FM_ERR_CUDA, "error-flag allocation failed");
+  }
   fm_status s = c64 ? init_tables<double>(P) : init_tables<float>(P);
   if (s != FM_OK) {
     fm_plan_destroy(P);
@@ -1091,7 +1132,7 @@ void fm_plan_destroy(fm_plan* P) {
                     &P->rzm, &P->V, &P->t1, &P->t2, &P->bbuf, &P->xbuf, &P->ebuf, &P->sbuf, &P->basis,
                     &P->gbuf2, &P->red_part, &P->red_out, &P->red_cnt, &P->active, &P->scale, &P->coef,
                     &P->hbuf, &P->eps_dev, &P->fx, &P->fy, &P->fz, &P->maxpart, &P->maxout, &P->wt_x,
-                    &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho};
+                    &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho, &P->errbuf};
   for (DevBuf* b : bufs) b->release();
   tk_resolve(P);
   for (cudaEvent_t e : P->evpool) cudaEventDestroy(e);
@@ -1163,7 +1204,7 @@ static fm_status apply_host(fm_plan* P, int nrhs, const double* x, double* y, in
                        nullptr));
   }
   FM_TRY(d2h_field<R>(P, P->ebuf.p, cnt, 1.0, y));
-  return FM_OK;
+  return check_device_error(P);
 }
 
 fm_status fm_green_apply(fm_plan* P, int nrhs, const double* x, double* y) {

@@ -26,6 +26,16 @@ cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, con
                       const double* rhs_scale, const EpiParams& ep, const void* twx, const void* rampx, void* out,
                       const int* active, cudaStream_t st);
 
+// TMA-staged y and z passes (fm_passes_tma.cuh).  They return cudaErrorNotSupported when the
+// shape has no TMA variant (the caller then uses the register-only passes).  `err` receives a
+// non-zero code if a pipeline wait timed out.
+template <typename S, typename R>
+cudaError_t launch_y_tma(const Dims& d, int dir, const void* in, const void* twy, const void* rampy, void* out,
+                         const int* active, int* err, int sms, cudaStream_t st);
+template <typename S, typename R>
+cudaError_t launch_zg_tma(const Dims& d, int mode, const void* in, const GreenParams& gp, const void* twz,
+                          const void* rz, void* out, const int* active, int* err, int sms, cudaStream_t st);
+
 // pencils that share one warp for an axis of length L (y/z passes need nx to be a multiple)
 template <typename R>
 int pencils_per_warp(int L);

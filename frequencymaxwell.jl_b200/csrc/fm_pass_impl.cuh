@@ -1,6 +1,7 @@
 // Launcher bodies for the axis passes; included once per precision.
 #pragma once
 #include "fm_launch.h"
+#include "fm_passes_tma.cuh"
 
 namespace fm {
 
@@ -160,6 +161,148 @@ cudaError_t launch_zg(const Dims& d, int mode, const void* in, const GreenParams
 #undef ZA
 #undef ZO
 #undef ZC
+}
+
+// ---- TMA tensor maps ----------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// Field batch viewed as 8-byte elements (one complex64, or half a complex128).
+// rank 3: (x, y, z*3*nb)  box (128 B, by, 1)      -- y pencils
+// rank 4: (x, y, z, 3*nb) box (128 B, 1, bz, 3)   -- z pencils, all components
+static bool make_map(CUtensorMap* m, void* base, const Dims& d, int esz, int rank, int box_y, int box_z) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const int w = esz / 8;  // 8-byte words per complex value
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4], es[4] = {1, 1, 1, 1};
+  dims[0] = (cuuint64_t)d.nx * w;
+  dims[1] = (cuuint64_t)d.ny;
+  strides[0] = (cuuint64_t)d.nx * esz;
+  strides[1] = (cuuint64_t)d.nx * d.ny * esz;
+  box[0] = 16;
+  if (rank == 3) {
+    dims[2] = (cuuint64_t)d.nz * 3 * d.nb;
+    box[1] = (cuuint32_t)box_y;
+    box[2] = 1;
+  } else {
+    dims[2] = (cuuint64_t)d.nz;
+    dims[3] = (cuuint64_t)3 * d.nb;
+    strides[2] = (cuuint64_t)d.n * esz;
+    box[1] = 1;
+    box[2] = (cuuint32_t)box_z;
+    box[3] = 3;
+  }
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, base, dims, strides, box, es,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename K>
+static unsigned persistent_grid(K kern, int threads, size_t smem, long long ntiles, int sms) {
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem) != cudaSuccess || bps < 1) bps = 1;
+  long long g = (long long)sms * bps;
+  if (g > ntiles) g = ntiles;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+template <typename S, typename R, int L, int DIR>
+static cudaError_t y_tma_L(const Dims& d, const void* in, const void* tw, const void* ramp, void* out, const int* act,
+                           int* err, int sms, cudaStream_t st) {
+  using C = YTmaCfg<S, R, L>;
+  if (d.nx % C::TX) return cudaErrorNotSupported;
+  CUtensorMap mi, mo;
+  const int box = L > 256 ? 256 : L;
+  if (!make_map(&mi, const_cast<void*>(in), d, (int)sizeof(cplx<S>), 3, box, 1) ||
+      !make_map(&mo, out, d, (int)sizeof(cplx<S>), 3, box, 1))
+    return cudaErrorNotSupported;
+  const size_t smem = C::SM::total;
+  allow_smem(k_y_tma<S, R, L, DIR>, smem);
+  const long long ntiles = (long long)(d.nx / C::TX) * d.nz * 3 * d.nb;
+  const unsigned grid = persistent_grid(k_y_tma<S, R, L, DIR>, C::THREADS, smem, ntiles, sms);
+  k_y_tma<S, R, L, DIR><<<grid, C::THREADS, smem, st>>>(d, mi, mo, (const cplx<R>*)tw + 0, (const cplx<R>*)ramp, act,
+                                                         err);
+  return cudaGetLastError();
+}
+
+template <typename S, typename R, int L, int MODE>
+static cudaError_t zg_tma_L(const Dims& d, const void* in, const GreenParams& gp, const void* tw, const void* rz,
+                            void* out, const int* act, int* err, int sms, cudaStream_t st) {
+  using C = ZTmaCfg<S, R, L, MODE>;
+  if (d.nx % C::TX) return cudaErrorNotSupported;
+  CUtensorMap mi, mo;
+  if (!make_map(&mi, const_cast<void*>(in), d, (int)sizeof(cplx<S>), 4, 1, L) ||
+      !make_map(&mo, out, d, (int)sizeof(cplx<S>), 4, 1, L))
+    return cudaErrorNotSupported;
+  const size_t smem = C::SM::total;
+  allow_smem(k_zg_tma<S, R, L, MODE>, smem);
+  const long long ntiles = (long long)(d.nx / C::TX) * d.ny * d.nb;
+  const unsigned grid = persistent_grid(k_zg_tma<S, R, L, MODE>, C::THREADS, smem, ntiles, sms);
+  k_zg_tma<S, R, L, MODE><<<grid, C::THREADS, smem, st>>>(d, mi, mo, gp, (const cplx<R>*)tw, (const cplx<R>*)rz, act,
+                                                           err);
+  return cudaGetLastError();
+}
+
+template <typename S, typename R>
+cudaError_t launch_y_tma(const Dims& d, int dir, const void* in, const void* tw, const void* ramp, void* out,
+                         const int* act, int* err, int sms, cudaStream_t st) {
+  // the table argument is the [forward | reversed] pair; the kernel picks its half
+#define YT(LL) (dir < 0 ? y_tma_L<S, R, LL, -1>(d, in, tw, ramp, out, act, err, sms, st) \
+                        : y_tma_L<S, R, LL, +1>(d, in, tw, ramp, out, act, err, sms, st))
+  switch (d.ny) {
+    case 32: return YT(32);
+    case 64: return YT(64);
+    case 128: return YT(128);
+    case 256: return YT(256);
+    default: return cudaErrorNotSupported;
+  }
+#undef YT
+}
+
+template <typename S, typename R>
+cudaError_t launch_zg_tma(const Dims& d, int mode, const void* in, const GreenParams& gp, const void* tw,
+                          const void* rz, void* out, const int* act, int* err, int sms, cudaStream_t st) {
+#define ZT(LL, M) zg_tma_L<S, R, LL, M>(d, in, gp, tw, rz, out, act, err, sms, st)
+  if (mode == ZMODE_AVG2) {
+    switch (d.nz) {
+      case 32: return ZT(32, ZMODE_AVG2);
+      case 64: return ZT(64, ZMODE_AVG2);
+      case 128: return ZT(128, ZMODE_AVG2);
+      default: return cudaErrorNotSupported;
+    }
+  }
+  if (mode == ZMODE_ONE) {
+    switch (d.nz) {
+      case 32: return ZT(32, ZMODE_ONE);
+      case 64: return ZT(64, ZMODE_ONE);
+      case 128: return ZT(128, ZMODE_ONE);
+      default: return cudaErrorNotSupported;
+    }
+  }
+  switch (d.nz) {
+    case 32: return ZT(32, ZMODE_CURL);
+    case 64: return ZT(64, ZMODE_CURL);
+    case 128: return ZT(128, ZMODE_CURL);
+    default: return cudaErrorNotSupported;
+  }
+#undef ZT
 }
 
 template <typename R>
