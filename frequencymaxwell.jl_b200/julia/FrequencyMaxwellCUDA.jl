@@ -1,0 +1,149 @@
+# FrequencyMaxwellCUDA.jl -- Julia binding of libfmcuda (C ABI in include/fmcuda.h).
+#
+# Source only: Julia is not available where this repository is built and tested, so this file is
+# not executed here.  It shows the ccall layer a FrequencyMaxwell.jl maintainer adds so that
+# `ConvergentBornSolver(...; device = :fmcuda)` routes `solve(solver, sources, medium)` to the GPU.
+module FrequencyMaxwellCUDA
+
+using FrequencyMaxwell
+using KernelAbstractions
+using LinearSolve
+
+const libfmcuda = get(ENV, "FMCUDA_LIB", joinpath(@__DIR__, "..", "fmcuda", "libfmcuda.so"))
+
+# Marker backend stored in solver.backend (convergent_born.jl:99); the device plugin point is
+# GPU_BACKENDS / register_gpu_backend! (FrequencyMaxwell.jl:127-140).
+struct FMCUDABackend <: KernelAbstractions.Backend end
+
+const FM_OK = Cint(0)
+const FM_NOT_CONVERGED = Cint(3)
+const FM_PREC_F64 = Cint(0)
+const FM_PREC_F32 = Cint(1)
+const FM_PREC_F32_MATH64 = Cint(2)
+
+struct FMPlanDesc
+    grid::NTuple{3,Cint}
+    pad::NTuple{3,Cint}
+    resolution::NTuple{3,Cdouble}
+    absorbing::NTuple{3,Cint}
+    precision::Cint
+    max_rhs::Cint
+    device::Cint
+end
+
+struct FMSolveOpts
+    method::Cint
+    ortho::Cint
+    restart::Cint
+    maxiters::Cint
+    reltol::Cdouble
+    abstol::Cdouble
+    timeout_s::Cdouble
+end
+
+struct FMSolveInfo
+    iterations::Cint
+    solved::Cint
+    residual::Cdouble
+    residual0::Cdouble
+end
+
+struct FMPotentialInfo
+    eps_imag::Cdouble
+    k_bg::Cdouble
+    bornmax::Cint
+end
+
+struct FMPlaneWave
+    wavelength::Cdouble
+    polarization::NTuple{6,Cdouble}
+    k_vector::NTuple{3,Cdouble}
+    amplitude::Cdouble
+    phase::Cdouble
+end
+
+function check(status)
+    status == FM_OK && return status
+    msg = unsafe_string(ccall((:fm_last_error, libfmcuda), Cstring, ()))
+    status == Cint(1) && throw(ArgumentError(msg))
+    status == FM_NOT_CONVERGED && return status
+    error("libfmcuda: " * msg)
+end
+
+function plan_desc(solver::ConvergentBornSolver{T}) where {T}
+    bcs = solver.boundary_conditions
+    pad = ntuple(i -> FrequencyMaxwell.padding_pixels(bcs[i], solver.resolution[i]), 3)
+    prec = T === Float64 ? FM_PREC_F64 : FM_PREC_F32_MATH64
+    FMPlanDesc(Cint.(solver.grid_size), Cint.(pad), Cdouble.(solver.resolution),
+               ntuple(i -> Cint(FrequencyMaxwell.requires_averaging(bcs[i])), 3), prec, Cint(1), Cint(0))
+end
+
+# the per-axis filters of _apply_attenuation_to_potential! (convergent_born.jl:893-944)
+function attenuation_filter(solver, dim)
+    bc = solver.boundary_conditions[dim]
+    pad = FrequencyMaxwell.padding_pixels(bc, solver.resolution[dim])
+    n = solver.grid_size[dim] + 2pad
+    (FrequencyMaxwell.requires_padding(bc) && pad > 0) || return ones(Float64, n)
+    L = min(pad, round(Int, bc.attenuation_thickness / (solver.resolution[dim] * 2)))
+    w = FrequencyMaxwell._create_attenuation_window(bc.profile, L, Float64) .* bc.sharpness .+ (1 - bc.sharpness)
+    return vcat(w, ones(Float64, solver.grid_size[dim] + 2 * (pad - L)), reverse(w))
+end
+
+"""
+    solve_fmcuda(solver, sources, medium) -> ElectromagneticField
+
+`solve(solver, sources, medium)` (convergent_born.jl:565-600) on libfmcuda.  A maintainer adds, as the
+first line of that method,
+
+    solver.backend isa FrequencyMaxwellCUDA.FMCUDABackend &&
+        return FrequencyMaxwellCUDA.solve_fmcuda(solver, sources, medium)
+"""
+function solve_fmcuda(solver::ConvergentBornSolver{T}, sources, medium) where {T}
+    FrequencyMaxwell.grid_size(medium) == solver.grid_size ||
+        throw(ArgumentError("medium grid_size must match solver grid_size"))
+    srcs = sources isa AbstractVector ? sources : [sources]
+    wavelength = FrequencyMaxwell.source_wavelength(sources)
+    desc = Ref(plan_desc(solver))
+    plan = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:fm_plan_create, libfmcuda), Cint, (Ref{FMPlanDesc}, Ref{Ptr{Cvoid}}), desc, plan))
+    try
+        eps = ComplexF64.(FrequencyMaxwell.permittivity(medium))
+        fx, fy, fz = (attenuation_filter(solver, d) for d in 1:3)
+        pinfo = Ref{FMPotentialInfo}()
+        check(ccall((:fm_build_potential, libfmcuda), Cint,
+                    (Ptr{Cvoid}, Ptr{ComplexF64}, Cdouble, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Cint,
+                     Ref{FMPotentialInfo}),
+                    plan[], eps, FrequencyMaxwell.permittivity_bg(medium), wavelength, fx, fy, fz,
+                    solver.iterations_max, pinfo))
+        bornmax = Int(pinfo[].bornmax)
+        bornmax >= 1 || throw(ArgumentError("Bornmax < 1"))
+        waves = [FMPlaneWave(s.wavelength,
+                             (real(s.polarization[1]), imag(s.polarization[1]), real(s.polarization[2]),
+                              imag(s.polarization[2]), real(s.polarization[3]), imag(s.polarization[3])),
+                             Tuple(Float64.(s.k_vector)), s.amplitude, s.phase) for s in srcs]
+        first = Cint[0, length(waves)]
+        method = solver.linear_solver isa LinearSolve.KrylovJL && occursin("bicgstab", lowercase(string(solver.linear_solver.KrylovAlg))) ? Cint(1) : Cint(0)
+        opts = Ref(FMSolveOpts(method, T === Float64 ? Cint(0) : Cint(1), Cint(0), Cint(max(2bornmax, 100)),
+                               solver.tolerance, solver.tolerance * 1e-2, 0.0))
+        E = Array{ComplexF64}(undef, solver.grid_size..., 3)
+        H = similar(E)
+        info = Ref{FMSolveInfo}()
+        st = check(ccall((:fm_solve_plane_waves, libfmcuda), Cint,
+                         (Ptr{Cvoid}, Cint, Ptr{Cint}, Ptr{FMPlaneWave}, Cdouble, Ref{FMSolveOpts}, Ptr{ComplexF64},
+                          Ptr{ComplexF64}, Ref{FMSolveInfo}),
+                         plan[], Cint(1), first, waves, FrequencyMaxwell.permittivity_bg(medium), opts, E, H, info))
+        st == FM_NOT_CONVERGED && @warn "LinearSolve.jl did not converge."
+        solver.Bornmax = bornmax
+        solver.iteration_count = info[].iterations
+        push!(solver.residual_history, T(info[].residual))
+        return ElectromagneticField(Complex{T}.(E), Complex{T}.(H), solver.resolution, wavelength)
+    finally
+        ccall((:fm_plan_destroy, libfmcuda), Cvoid, (Ptr{Cvoid},), plan[])
+    end
+end
+
+function __init__()
+    FrequencyMaxwell.register_gpu_backend!(:fmcuda, () -> FMCUDABackend())
+end
+
+end # module
