@@ -30,7 +30,7 @@ EXPORTED = (
     "fm_abi_version", "fm_last_error", "fm_device_count", "fm_plan_create", "fm_plan_destroy", "fm_plan_bytes",
     "fm_set_potential", "fm_green_apply", "fm_apply_operator", "fm_apply_preconditioner", "fm_curl_field",
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
-    "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream",
+    "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream", "fm_green_apply_noalloc",
 )
 
 
@@ -106,6 +106,8 @@ def lib() -> C.CDLL:
     L.fm_kernel_stats.restype = C.c_int
     L.fm_launch_count.argtypes = [P]
     L.fm_launch_count.restype = C.c_longlong
+    L.fm_green_apply_noalloc.argtypes = [C.POINTER(fm_plan_desc), C.c_double, C.c_double, C.c_int, P, P, P]
+    L.fm_green_apply_noalloc.restype = C.c_int
     L.fm_stream.argtypes = [P]
     L.fm_stream.restype = C.c_void_p
     for name in ("fm_plan_create", "fm_set_potential", "fm_green_apply", "fm_apply_operator",

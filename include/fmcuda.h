@@ -159,6 +159,21 @@ fm_status fm_copy_fields(fm_plan* plan, int nrhs, double* E_out, double* H_out);
 /* Wait for the plan's stream. */
 fm_status fm_synchronize(fm_plan* plan);
 
+/* ---- Green application without device allocation ----------------------
+ * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc (their own
+ * pooled allocator, a fixed device-memory budget, a loop that must not touch the allocator): the
+ * Green application conv!(G, x) of fm_green_apply on device buffers the caller owns, with no plan.
+ * x_dev and y_dev hold nrhs fields in the storage type of desc->precision (complex128 for
+ * FM_PREC_F64, complex64 otherwise), laid out as above; they must not overlap (y doubles as a pass
+ * temporary).  desc gives grid, padding, resolution, boundaries, precision and device; max_rhs is
+ * ignored.  The only scratch is one static 64 MiB device array per GPU that loads the library
+ * (tables, an error flag and one field-sized temporary), so sizes whose temporary does not fit are
+ * rejected with FM_ERR_INVALID.  The first call on a device looks up that array's address and should
+ * come before any stream capture.  Calls share the array: calls that overlap on the GPU race.  Work is
+ * issued on `stream` (NULL: default stream) and the call returns after it has finished. */
+fm_status fm_green_apply_noalloc(const fm_plan_desc* desc, double k_bg, double eps_imag, int nrhs, const void* x_dev,
+                                 void* y_dev, void* stream);
+
 /* ---- instrumentation (no reference counterpart: measurement support) ---- */
 
 typedef struct {
