@@ -49,35 +49,9 @@ METRIC = "solves/s at rel-L2<=1e-5 vs FP64: batched FP32 vs plain FP64; p50/p99 
 def batching_sources(n_angles=32, seed=SEED):
     """32 (kx, ky) uniform in the NA 1.2 disk (sin(theta) <= NA/n_bg), snapped to the lattice
     2*pi*m/(N*dx); polarisations s and p (two unit vectors orthogonal to k)."""
-    rng = np.random.default_rng(seed + 1)
-    nbg = math.sqrt(EPS_BG)
-    kbg = 2 * math.pi * nbg / WL
-    out = []
-    dk = [2 * math.pi / (GRID[d] * RES[d]) for d in range(2)]
-    while len(out) < n_angles:
-        r = math.sqrt(rng.uniform()) * NA / nbg
-        phi = rng.uniform(0, 2 * math.pi)
-        kx, ky = kbg * r * math.cos(phi), kbg * r * math.sin(phi)
-        kx = round(kx / dk[0]) * dk[0]
-        ky = round(ky / dk[1]) * dk[1]
-        st = math.hypot(kx, ky) / kbg
-        if st > NA / nbg:
-            continue
-        kz = math.sqrt(max(0.0, 1 - st * st))
-        k = np.array([kx / kbg, ky / kbg, kz])
-        k /= np.linalg.norm(k)
-        out.append(k)
-    pols = []
-    for k in out:
-        s = np.cross(k, [0.0, 0.0, 1.0])
-        if np.linalg.norm(s) < 1e-12:
-            s = np.array([0.0, 1.0, 0.0])
-        s /= np.linalg.norm(s)
-        p = np.cross(s, k)
-        p /= np.linalg.norm(p)
-        pols.append((k, s))
-        pols.append((k, p))
-    return pols
+    import fmcuda as F
+    return [(s.k_vector, s.polarization.real) for s in
+            F.illumination_cone(GRID, RES, WL, EPS_BG, n_angles, NA, seed)]
 
 
 def make_inputs():
@@ -324,6 +298,10 @@ def run(args):
                    "GBps": round(v["bytes"] / (v["ms"] / 1000) / 1e9, 1) if v["ms"] > 0 else None}
                for k, v in kstats.items() if v["launches"]}
 
+    solver.release()
+    serving = None
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        serving = run_serving(args)
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_baseline()
@@ -349,13 +327,33 @@ def run(args):
                         "d2h_bytes_per_step": d2h},
                 "roofline": roof, "kernel_classes": classes,
                 "algorithmic_GBps_all_kernels": all_bytes / (total_ms / 1000) / 1e9 if total_ms else None,
-                "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
+                "serving": serving, "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(line))
-    solver.release()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def run_serving(args):
+    """Continuous batching of a seeded Poisson request stream (bounded sample of the serving workload):
+    grids drawn uniformly from {64x64x32, 96x96x64, 128x128x64, 256x256x128}, 1-32 angles each, 12-bead
+    phantoms, complex64 fields with FP64 dots, tolerance 1e-5, slots sized from a 150 GB device budget."""
+    from fmcuda import serving as SV
+    reqs = SV.serving_requests(args.serving_requests, rate=args.serving_rate, seed=SEED)
+    srv = SV.Server(SV.SERVING_SHAPES, budget_bytes=args.serving_budget_gb * 1e9, basis=args.serving_basis,
+                    precision=args.precision)
+    try:
+        srv.start()
+        rep = SV.run_stream(srv, reqs, timeout=1800)
+    finally:
+        srv.stop()
+    rep.update({"budget_GB": args.serving_budget_gb, "basis": args.serving_basis, "tolerance": 1e-5,
+                "rate_req_per_s": args.serving_rate, "shapes": ["x".join(map(str, s)) for s in SV.SERVING_SHAPES],
+                "latency": "request arrival to its last right-hand side's fields on the host",
+                "iterations": {"min": min(i["iterations"] for r in reqs for i in r.infos.values()),
+                               "max": max(i["iterations"] for r in reqs for i in r.infos.values())}})
+    return rep
 
 
 def run_operator_case(args):
@@ -393,9 +391,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--operator-case", action="store_true", help="profiling case: operator applications only")
     ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--serving-requests", type=int, default=16, help="requests in the serving sample (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=200.0)
+    ap.add_argument("--serving-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serving-basis", type=int, default=100)
+    ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
     args = ap.parse_args()
     if args.operator_case:
         return run_operator_case(args)
+    if args.serving_only:
+        print(json.dumps({"serving": run_serving(args)}))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run(args)

@@ -35,6 +35,19 @@ __device__ __forceinline__ void bf4(T& v0, T& v1, T& v2, T& v3) {
   v3 = csub(t1, t3);
 }
 
+// radix 3: X_k = sum_n v_n w^(nk), w = exp(DIR*2*pi*i/3) = -1/2 + i*DIR*sin(pi/3)
+template <int DIR, typename T>
+__device__ __forceinline__ void bf3(T& a, T& b, T& c) {
+  using R = typename RealOf<T>::R;
+  const R h = R(0.5), s3 = R(0.86602540378443864676);
+  const T t1 = cadd(b, c), t2 = csub(b, c);
+  const T m1 = mk(a.x - h * t1.x, a.y - h * t1.y);
+  const T m2 = mk(-R(DIR) * s3 * t2.y, R(DIR) * s3 * t2.x);  // i*DIR*sin(pi/3)*(b - c)
+  a = cadd(a, t1);
+  b = cadd(m1, m2);
+  c = csub(m1, m2);
+}
+
 // multiply by exp(DIR * 2*pi*i*M/16)
 template <int DIR, int M, typename T>
 __device__ __forceinline__ T tw16(T a) {
@@ -99,6 +112,7 @@ __device__ __forceinline__ void bf16(T* v) {
 template <int DIR, int RAD, typename T>
 __device__ __forceinline__ void bfly(T* v) {
   if constexpr (RAD == 2) bf2<DIR>(v[0], v[1]);
+  else if constexpr (RAD == 3) bf3<DIR>(v[0], v[1], v[2]);
   else if constexpr (RAD == 4) bf4<DIR>(v[0], v[1], v[2], v[3]);
   else if constexpr (RAD == 8) bf8<DIR>(v);
   else if constexpr (RAD == 16) bf16<DIR>(v);
@@ -195,6 +209,7 @@ FM_PLAN(64, float, 8, 8, 8, 0)
 FM_PLAN(128, float, 16, 16, 8, 0)
 FM_PLAN(256, float, 16, 16, 16, 0)
 FM_PLAN(512, float, 16, 16, 8, 4)
+FM_PLAN(96, float, 24, 8, 4, 3)
 FM_PLAN(8, double, 2, 2, 2, 2)
 FM_PLAN(16, double, 4, 4, 4, 0)
 FM_PLAN(32, double, 8, 8, 4, 0)
@@ -202,6 +217,7 @@ FM_PLAN(64, double, 8, 8, 8, 0)
 FM_PLAN(128, double, 8, 8, 4, 4)
 FM_PLAN(256, double, 8, 8, 8, 4)
 FM_PLAN(512, double, 16, 16, 8, 4)
+FM_PLAN(96, double, 24, 8, 4, 3)
 #undef FM_PLAN
 
 // forward-order run (radices R0, R1, R2) with its stage-twiddle table

@@ -51,11 +51,14 @@ __device__ __forceinline__ void finish_reduce(double2* part, double2* out, unsig
 }
 
 // out[b][i] = sum_e conj(U_i[b][e]) * w[b][e]   (i < K), plus out[b][K] = ||w||^2 when WNORM.
+// Optional per-RHS arguments: wtab[b] replaces w + b*M, Kb[b] (<= K) the number of basis vectors.
 template <typename R, bool WNORM>
 __global__ void __launch_bounds__(KV_THREADS) k_multidot(long long M, int B, int K, const cplx<R>* __restrict__ U,
                                                          const cplx<R>* __restrict__ w, double2* __restrict__ part,
                                                          double2* __restrict__ out, unsigned* __restrict__ counter,
-                                                         const int* __restrict__ active) {
+                                                         const int* __restrict__ active,
+                                                         const cplx<R>* const* __restrict__ wtab = nullptr,
+                                                         const int* __restrict__ Kb = nullptr) {
   using T = cplx<R>;
   __shared__ double2 acc[KV_WARPS][KV_KMAX + 1];
   const int b = blockIdx.y, nblk = gridDim.x;
@@ -67,7 +70,8 @@ __global__ void __launch_bounds__(KV_THREADS) k_multidot(long long M, int B, int
   const long long chunk = (long long)KV_THREADS * KV_EPT;
   const long long per = ((M + nblk - 1) / nblk + chunk - 1) / chunk * chunk;
   const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
-  const T* wb = w + (size_t)b * M;
+  const T* wb = wtab ? wtab[b] : w + (size_t)b * M;
+  const int Kr = Kb ? Kb[b] : K;
   for (long long c0 = lo; c0 < hi; c0 += chunk) {
     double2 wv[KV_EPT];
 #pragma unroll
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_multidot(long long M, int B, int
       long long e = c0 + (long long)k * KV_THREADS + threadIdx.x;
       wv[k] = e < hi ? to_d(wb[e]) : make_double2(0.0, 0.0);
     }
-    for (int i = 0; i < K; ++i) {
+    for (int i = 0; i < Kr; ++i) {
       const T* ub = U + ((size_t)i * B + b) * M;
       double2 s = make_double2(0.0, 0.0);
 #pragma unroll
@@ -135,19 +139,22 @@ template <typename R, bool NORM>
 __global__ void __launch_bounds__(KV_THREADS) k_update(long long M, int B, int K, const cplx<R>* __restrict__ U,
                                                        Coef cf, cplx<R>* __restrict__ w, const double* __restrict__ w_scale,
                                                        double2* __restrict__ part, double2* __restrict__ out,
-                                                       unsigned* __restrict__ counter, const int* __restrict__ active) {
+                                                       unsigned* __restrict__ counter, const int* __restrict__ active,
+                                                       cplx<R>* const* __restrict__ wtab = nullptr,
+                                                       const int* __restrict__ Kb = nullptr) {
   using T = cplx<R>;
   __shared__ double2 cs[KV_KMAX];
   __shared__ double red[KV_WARPS];
   const int b = blockIdx.y, nblk = gridDim.x;
   if (active && !active[b]) return;
-  for (int i = threadIdx.x; i < K; i += blockDim.x) cs[i] = cf.get(b, i);
+  const int Kr = Kb ? Kb[b] : K;
+  for (int i = threadIdx.x; i < Kr; i += blockDim.x) cs[i] = cf.get(b, i);
   __syncthreads();
   const double a0 = w_scale ? w_scale[b] : 1.0;
   const long long chunk = (long long)KV_THREADS * KV_EPT;
   const long long per = ((M + nblk - 1) / nblk + chunk - 1) / chunk * chunk;
   const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
-  T* wb = w + (size_t)b * M;
+  T* wb = wtab ? wtab[b] : w + (size_t)b * M;
   double nrm = 0.0;
   for (long long c0 = lo; c0 < hi; c0 += chunk) {
     double2 acc[KV_EPT];
@@ -157,7 +164,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_update(long long M, int B, int K
       double2 v = e < hi ? to_d(wb[e]) : make_double2(0.0, 0.0);
       acc[k] = make_double2(v.x * a0, v.y * a0);
     }
-    for (int i = 0; i < K; ++i) {
+    for (int i = 0; i < Kr; ++i) {
       const T* ub = U + ((size_t)i * B + b) * M;
       const double2 c = cs[i];
 #pragma unroll

@@ -10,11 +10,13 @@ namespace fm {
 // Largest supported axis length and the largest z length with the averaged
 // (length-2L) transform.
 constexpr int AXIS_MAX = 512;
+// axis lengths with an FFT plan: powers of two in [8, AXIS_MAX] and 96 (radices 8, 4, 3)
+inline bool axis_supported(int n) { return (n >= 8 && n <= AXIS_MAX && (n & (n - 1)) == 0) || n == 96; }
 constexpr int AXIS_MAX_AVG2 = 256;
 
 template <typename S, typename R>
 cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, const double* rhs_scale, const void* twx,
-                      const void* rampx, void* out, const int* active, cudaStream_t st);
+                      const void* rampx, void* out, const int* active, cudaStream_t st, VecTab vt = VecTab{});
 template <typename S, typename R>
 cudaError_t launch_y(const Dims& d, int dir, const void* in, const void* twy, const void* rampy, void* out,
                      const int* active, cudaStream_t st);
@@ -24,7 +26,7 @@ cudaError_t launch_zg(const Dims& d, int mode, const void* in, const GreenParams
 template <typename S, typename R>
 cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
                       const double* rhs_scale, const EpiParams& ep, const void* twx, const void* rampx, void* out,
-                      const int* active, cudaStream_t st);
+                      const int* active, cudaStream_t st, VecTab vt = VecTab{});
 
 // TMA-staged y and z passes (fm_passes_tma.cuh).  They return cudaErrorNotSupported when the
 // shape has no TMA variant (the caller then uses the register-only passes).  `err` receives a

@@ -3,14 +3,14 @@
 
 namespace fm {
 template cudaError_t launch_xf<double, double>(const Dims&, int, const void*, const void*, const double*, const void*,
-                                      const void*, void*, const int*, cudaStream_t);
+                                      const void*, void*, const int*, cudaStream_t, VecTab);
 template cudaError_t launch_y<double, double>(const Dims&, int, const void*, const void*, const void*, void*, const int*,
                                      cudaStream_t);
 template cudaError_t launch_zg<double, double>(const Dims&, int, const void*, const GreenParams&, const void*, const void*,
                                       void*, const int*, cudaStream_t);
 template cudaError_t launch_xi<double, double>(const Dims&, int, const void*, const void*, const void*, const void*,
                                       const double*, const EpiParams&, const void*, const void*, void*, const int*,
-                                      cudaStream_t);
+                                      cudaStream_t, VecTab);
 template int pencils_per_warp<double>(int);
 template cudaError_t launch_y_tma<double, double>(const Dims&, int, const void*, const void*, const void*, void*,
                                           const int*, int*, int, cudaStream_t);

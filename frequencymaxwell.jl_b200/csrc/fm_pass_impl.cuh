@@ -15,7 +15,7 @@ constexpr int ZG_THREADS = 128;
 
 template <typename S, typename R, int L, int PRO>
 static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const double* rs, const void* tw, const void* ramp,
-                        void* out, const int* act, cudaStream_t st) {
+                        void* out, const int* act, cudaStream_t st, const VecTab& vt) {
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
@@ -26,14 +26,14 @@ static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const doub
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xf<S, R, L, PRO>, smem);
   k_xf<S, R, L, PRO><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, rs, (const T*)tw,
-                                                         (const T*)ramp, (TS*)out, act);
+                                                         (const T*)ramp, (TS*)out, act, vt);
   return cudaGetLastError();
 }
 
 template <typename S, typename R, int L, int EPI>
 static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void* xv, const void* bv, const double* rs,
                         const EpiParams& ep, const void* tw, const void* ramp, void* out, const int* act,
-                        cudaStream_t st) {
+                        cudaStream_t st, const VecTab& vt) {
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
@@ -44,7 +44,7 @@ static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xi<S, R, L, EPI>, smem);
   k_xi<S, R, L, EPI><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, (const TS*)bv,
-                                                         rs, ep, (const T*)tw, (const T*)ramp, (TS*)out, act);
+                                                         rs, ep, (const T*)tw, (const T*)ramp, (TS*)out, act, vt);
   return cudaGetLastError();
 }
 
@@ -89,13 +89,14 @@ static cudaError_t zg_L(const Dims& d, const void* in, const GreenParams& gp, co
     case 128: return EXPR(128);                     \
     case 256: return EXPR(256);                     \
     case 512: return EXPR(512);                     \
+    case 96: return EXPR(96);                       \
     default: return cudaErrorInvalidValue;          \
   }
 
 template <typename S, typename R>
 cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, const double* rs, const void* tw,
-                      const void* ramp, void* out, const int* act, cudaStream_t st) {
-#define XF_(LL, P) xf_L<S, R, LL, P>(d, in, V, rs, tw, ramp, out, act, st)
+                      const void* ramp, void* out, const int* act, cudaStream_t st, VecTab vt) {
+#define XF_(LL, P) xf_L<S, R, LL, P>(d, in, V, rs, tw, ramp, out, act, st, vt)
 #define XF0(LL) XF_(LL, PRO_COPY)
 #define XF1(LL) XF_(LL, PRO_V)
 #define XF2(LL) XF_(LL, PRO_V_SCALE)
@@ -111,8 +112,8 @@ cudaError_t launch_xf(const Dims& d, int pro, const void* in, const void* V, con
 template <typename S, typename R>
 cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
                       const double* rs, const EpiParams& ep, const void* tw, const void* ramp, void* out,
-                      const int* act, cudaStream_t st) {
-#define XI_(LL, E) xi_L<S, R, LL, E>(d, in, V, xv, bv, rs, ep, tw, ramp, out, act, st)
+                      const int* act, cudaStream_t st, VecTab vt) {
+#define XI_(LL, E) xi_L<S, R, LL, E>(d, in, V, xv, bv, rs, ep, tw, ramp, out, act, st, vt)
 #define XI0(LL) XI_(LL, EPI_STORE)
 #define XI1(LL) XI_(LL, EPI_OP)
 #define XI2(LL) XI_(LL, EPI_PREC_OP)
@@ -267,6 +268,7 @@ cudaError_t launch_y_tma(const Dims& d, int dir, const void* in, const void* tw,
 #define YT(LL) (dir < 0 ? y_tma_L<S, R, LL, -1>(d, in, tw, ramp, out, act, err, sms, st) \
                         : y_tma_L<S, R, LL, +1>(d, in, tw, ramp, out, act, err, sms, st))
   switch (d.ny) {
+    case 96: return YT(96);
     case 32: return YT(32);
     case 64: return YT(64);
     case 128: return YT(128);
@@ -315,6 +317,7 @@ int pencils_per_warp(int L) {
     case 128: return 32 / Plan<128, R>::TP;
     case 256: return 32 / Plan<256, R>::TP;
     case 512: return 32 / Plan<512, R>::TP;
+    case 96: return 32 / Plan<96, R>::TP;
     default: return 0;
   }
 }

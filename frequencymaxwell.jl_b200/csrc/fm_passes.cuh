@@ -26,7 +26,14 @@ __device__ __forceinline__ To cv(From a) {
 
 struct Dims {
   int nx, ny, nz, nb;
-  long long n;  // nx*ny*nz
+  long long n;           // nx*ny*nz
+  long long vstride = 0; // potential of RHS b at V + b*vstride (0: one potential shared by all RHS)
+};
+
+// Optional per-RHS vector pointers (RHS b's field starts at tab[b]); null -> contiguous batch.
+struct VecTab {
+  const void* const* in = nullptr;   // XF input / XI operator input x
+  void* const* out = nullptr;        // XI output
 };
 
 // Warp-local exchange buffers: each warp owns PW pencils of STRIDE elements.
@@ -54,7 +61,7 @@ template <typename S, typename R, int L, int PRO>
 __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
                                             const double* __restrict__ rhs_scale, const cplx<R>* __restrict__ twx,
                                             const cplx<R>* __restrict__ rampx, cplx<S>* __restrict__ out,
-                                            const int* __restrict__ active) {
+                                            const int* __restrict__ active, VecTab vt) {
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
@@ -76,18 +83,20 @@ __global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<S>* __restrict__ 
   T vrow[E];
   if constexpr (PRO != PRO_COPY) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) vrow[e] = cv<T>(V[yz * L + lay_idx<L, E, P_::R0>(t, e)]);
+    for (int e = 0; e < E; ++e) vrow[e] = cv<T>(V[b * d.vstride + yz * L + lay_idx<L, E, P_::R0>(t, e)]);
   }
   R s = R(1);
   if constexpr (PRO == PRO_V_SCALE) s = (R)rhs_scale[b];
+  const cplx<S>* inb = vt.in ? (const cplx<S>*)vt.in[b] : in + (long long)b * 3 * d.n;
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
     const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
+    const long long rbase = ((long long)c * d.ny * d.nz + yz) * L;
     T v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int x = lay_idx<L, E, P_::R0>(t, e);
-      T a = cv<T>(in[base + x]);
+      T a = cv<T>(inb[rbase + x]);
       if constexpr (PRO != PRO_COPY) a = cmul(a, vrow[e]);
       if constexpr (PRO == PRO_V_SCALE) a = cscale(a, s);
       if (rampx) a = cmul(a, rampx[x]);
@@ -176,6 +185,7 @@ struct GreenParams {
   double ksq_re, ksq_im;  // k_square / k_ref^2
   double scale_re, scale_im;  // folded normalisation (and curl factor)
   int curl_index;    // 1 -> curl index formula for odd sizes
+  const double* ksq_im_b = nullptr;  // per-RHS imaginary part of k_square (null: ksq_im for all)
 };
 
 template <typename R>
@@ -248,7 +258,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
       kx = (R)gp.dk[0] * (kidx_green<R>(kxi, d.nx) + (R)gp.shift[0]);
       ky = (R)gp.dk[1] * (kidx_green<R>(kyi, d.ny) + (R)gp.shift[1]);
     }
-    const R ksr = (R)gp.ksq_re, ksi = (R)gp.ksq_im;
+    const R ksr = (R)gp.ksq_re, ksi = gp.ksq_im_b ? (R)gp.ksq_im_b[b] : (R)gp.ksq_im;
     const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
     // 1/k_square
     const R kden = ksr * ksr + ksi * ksi;
@@ -318,6 +328,7 @@ enum { EPI_STORE = 0, EPI_OP = 1, EPI_PREC_OP = 2, EPI_PREC_RES = 3 };
 struct EpiParams {
   double alpha_re, alpha_im, beta_re, beta_im;
   double inv_eps;  // 1/eps_imag (scaled units)
+  const double* inv_eps_b = nullptr;  // per-RHS 1/eps_imag (null: inv_eps for all)
 };
 
 template <typename S, typename R, int L, int EPI>
@@ -325,7 +336,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
                                             const cplx<S>* __restrict__ xv, const cplx<S>* __restrict__ bv,
                                             const double* __restrict__ rhs_scale, EpiParams ep,
                                             const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ rampx,
-                                            cplx<S>* __restrict__ out, const int* __restrict__ active) {
+                                            cplx<S>* __restrict__ out, const int* __restrict__ active, VecTab vt) {
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
@@ -346,19 +357,23 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
   T* sm = warp_smem<T, PencilStride<L, T, TP, true>::v>(ex, wic, PW, p);
   T gam[E];
   if constexpr (EPI == EPI_PREC_OP || EPI == EPI_PREC_RES) {
-    const R ie = (R)ep.inv_eps;
+    const R ie = ep.inv_eps_b ? (R)ep.inv_eps_b[b] : (R)ep.inv_eps;
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      T vv = cv<T>(V[yz * L + lay_idx<L, E, P_::R0>(t, e)]);
+      T vv = cv<T>(V[b * d.vstride + yz * L + lay_idx<L, E, P_::R0>(t, e)]);
       gam[e] = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
     }
   }
   R s = R(1);
   if (rhs_scale) s = (R)rhs_scale[b];
   const T al = mk((R)ep.alpha_re, (R)ep.alpha_im), be = mk((R)ep.beta_re, (R)ep.beta_im);
+  const cplx<S>* xvb = vt.in ? (const cplx<S>*)vt.in[b] : xv + (long long)b * 3 * d.n;
+  cplx<S>* outb = vt.out ? (cplx<S>*)vt.out[b] : out + (long long)b * 3 * d.n;
+  const cplx<S>* bvb = bv + (long long)b * 3 * d.n;
 #pragma unroll 1
   for (int c = 0; c < 3; ++c) {
     const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
+    const long long rbase = ((long long)c * d.ny * d.nz + yz) * L;
     T v[E];
 #pragma unroll
     for (int e = 0; e < E; ++e) v[e] = cv<T>(in[base + lay_idx<L, E, P_::RL>(t, e)]);
@@ -366,25 +381,25 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int x = lay_idx<L, E, P_::R0>(t, e);
-      const long long ix = base + x;
+      const long long ix = rbase + x;
       T g = v[e];
       if (rampx) g = cmul(g, cconj(rampx[x]));
       T r;
       if constexpr (EPI == EPI_STORE) {
         r = g;
       } else if constexpr (EPI == EPI_OP) {
-        T xx = cv<T>(xv[ix]);
+        T xx = cv<T>(xvb[ix]);
         T a = cmul(al, csub(xx, g));
-        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(out[ix])));
+        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(outb[ix])));
         r = a;
       } else if constexpr (EPI == EPI_PREC_OP) {
-        T xx = cscale(cv<T>(xv[ix]), s);
+        T xx = cscale(cv<T>(xvb[ix]), s);
         r = cmul(gam[e], csub(xx, g));
       } else {
-        T xx = cscale(cv<T>(xv[ix]), s);
-        r = cmul(gam[e], cadd(csub(cv<T>(bv[ix]), xx), g));
+        T xx = cscale(cv<T>(xvb[ix]), s);
+        r = cmul(gam[e], cadd(csub(cv<T>(bvb[ix]), xx), g));
       }
-      out[ix] = cv<TS>(r);
+      outb[ix] = cv<TS>(r);
     }
     __syncwarp();
   }

@@ -228,9 +228,7 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
   }
   const int p = lane / TP, t = lane % TP;
   T* sm = ex + (warp * PW + p) * C::STRIDE;
-  const R ksr = (R)gp.ksq_re, ksi = (R)gp.ksq_im;
-  const R kden = ksr * ksr + ksi * ksi;
-  const T iks = mk(ksr / kden, -ksi / kden);
+  const R ksr = (R)gp.ksq_re;
   const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
   int it = 0;
   bool ok = true;
@@ -243,6 +241,9 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
     const uint32_t ph = (it / NST) & 1;
     if (!mbar_wait(full + s, ph, err, 23)) { ok = false; break; }
     unsigned char* tl = tiles + s * C::TILE;
+    const R ksi = gp.ksq_im_b ? (R)gp.ksq_im_b[b] : (R)gp.ksq_im;
+    const R kden = ksr * ksr + ksi * ksi;
+    const T iks = mk(ksr / kden, -ksi / kden);
 #pragma unroll 1
     for (int rd = 0; rd < C::ROUNDS; ++rd) {
       const int xl = rd * CW * PW + warp * PW + p;

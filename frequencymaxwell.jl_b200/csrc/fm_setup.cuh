@@ -104,9 +104,11 @@ __device__ __forceinline__ void incident_at(const WaveTabs& w, const PadInfo& pi
 }
 
 // S[b] = (V + i eps') .* E_inc  in scaled units (V already scaled, eps_s = eps_imag * inv_kref2)
+// (vstride, eps_b): per-RHS potential V + b*vstride and eps_b[b] (0 / null: shared V, eps_s)
 template <typename R>
 __global__ void __launch_bounds__(256) k_source_term(PadInfo pi, int B, WaveTabs w, const cplx<R>* __restrict__ V,
-                                                      double eps_s, cplx<R>* __restrict__ S, const int* __restrict__ active) {
+                                                      double eps_s, cplx<R>* __restrict__ S, const int* __restrict__ active,
+                                                      long long vstride = 0, const double* __restrict__ eps_b = nullptr) {
   const long long n = (long long)pi.nx * pi.ny * pi.nz;
   const int b = blockIdx.y;
   if (active && !active[b]) return;
@@ -116,8 +118,8 @@ __global__ void __launch_bounds__(256) k_source_term(PadInfo pi, int B, WaveTabs
     const int z = (int)(i / ((long long)pi.nx * pi.ny));
     double2 E[3], H[3];
     incident_at(w, pi, b, x, y, z, E, H, false);
-    double2 v = to_d(V[i]);
-    v.y += eps_s;
+    double2 v = to_d(V[b * vstride + i]);
+    v.y += eps_b ? eps_b[b] : eps_s;
 #pragma unroll
     for (int c = 0; c < 3; ++c) S[((size_t)b * 3 + c) * n + i] = from_d<cplx<R>>(cmul(v, E[c]));
   }
@@ -127,10 +129,11 @@ __global__ void __launch_bounds__(256) k_source_term(PadInfo pi, int B, WaveTabs
 template <typename R>
 __global__ void __launch_bounds__(256) k_assemble(PadInfo pi, int B, WaveTabs w, const cplx<R>* __restrict__ Es,
                                                    const cplx<R>* __restrict__ Hs, double2* __restrict__ Eo,
-                                                   double2* __restrict__ Ho) {
+                                                   double2* __restrict__ Ho, const int* __restrict__ active = nullptr) {
   const long long n = (long long)pi.nx * pi.ny * pi.nz;
   const long long g = (long long)pi.gx * pi.gy * pi.gz;
   const int b = blockIdx.y;
+  if (active && !active[b]) return;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g; i += (long long)gridDim.x * blockDim.x) {
     const int ux = (int)(i % pi.gx);
     const int uy = (int)((i / pi.gx) % pi.gy);

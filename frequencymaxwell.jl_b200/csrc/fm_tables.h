@@ -48,6 +48,7 @@ inline std::vector<cd_t> twiddles(int L) {
     case 128: r = radices_of<128, R>(); break;
     case 256: r = radices_of<256, R>(); break;
     case 512: r = radices_of<512, R>(); break;
+    case 96: r = radices_of<96, R>(); break;
     default: break;
   }
   std::vector<cd_t> t(2 * (size_t)L, cd_t(1.0, 0.0));

@@ -12,7 +12,8 @@ from .medium import (AbstractMedium, Medium, grid_size, permittivity, permittivi
                      phantom_cylinder, phantom_plate, phantom_random_beads)
 from .solver import (BornSeries, ConvergentBornSolver, DevicePlan, KrylovJL_BICGSTAB, KrylovJL_GMRES, compute_ROI,
                      domain_size, grid_spacing, reset, solve, solve_batch)
-from .sources import AbstractCurrentSource, PlaneWaveSource, generate_incident_field, source_wavelength
+from .sources import (AbstractCurrentSource, PlaneWaveSource, generate_incident_field, illumination_cone,
+                      source_wavelength)
 from . import _lib
 
 __all__ = [n for n in dir() if not n.startswith("_")]

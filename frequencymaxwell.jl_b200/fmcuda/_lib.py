@@ -31,6 +31,8 @@ EXPORTED = (
     "fm_set_potential", "fm_green_apply", "fm_apply_operator", "fm_apply_preconditioner", "fm_curl_field",
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
     "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream", "fm_green_apply_noalloc",
+    "fm_engine_slot_bytes", "fm_engine_create", "fm_engine_destroy", "fm_engine_submit", "fm_engine_step",
+    "fm_engine_status",
 )
 
 
@@ -106,6 +108,19 @@ def lib() -> C.CDLL:
     L.fm_kernel_stats.restype = C.c_int
     L.fm_launch_count.argtypes = [P]
     L.fm_launch_count.restype = C.c_longlong
+    L.fm_engine_slot_bytes.argtypes = [C.POINTER(fm_plan_desc), C.c_int]
+    L.fm_engine_slot_bytes.restype = C.c_longlong
+    L.fm_engine_create.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, P, P, P, C.c_int, C.POINTER(P)]
+    L.fm_engine_create.restype = C.c_int
+    L.fm_engine_destroy.argtypes = [P]
+    L.fm_engine_destroy.restype = None
+    L.fm_engine_submit.argtypes = [P, C.c_longlong, P, C.c_int, C.POINTER(fm_plane_wave), C.c_double, C.c_int, P, P]
+    L.fm_engine_submit.restype = C.c_int
+    L.fm_engine_step.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                 C.POINTER(fm_solve_info), C.c_int]
+    L.fm_engine_step.restype = C.c_int
+    L.fm_engine_status.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.fm_engine_status.restype = C.c_int
     L.fm_green_apply_noalloc.argtypes = [C.POINTER(fm_plan_desc), C.c_double, C.c_double, C.c_int, P, P, P]
     L.fm_green_apply_noalloc.restype = C.c_int
     L.fm_stream.argtypes = [P]

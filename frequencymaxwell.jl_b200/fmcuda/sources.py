@@ -2,7 +2,7 @@
 from __future__ import annotations
 
 import math
-from typing import Sequence, Union
+from typing import List, Sequence, Union
 
 import numpy as np
 
@@ -98,3 +98,38 @@ def generate_incident_field(sources: Sources, solver, permittivity_bg: float = 1
             E[..., c] += amp * Ep[c]
             H[..., c] += amp * Hp[c]
     return ElectromagneticField(E, H, res, srcs[0].wavelength)
+
+
+def illumination_cone(grid_size, resolution, wavelength: float, permittivity_bg: float, n_angles: int, na: float,
+                      seed: int, polarizations: str = "sp") -> List[PlaneWaveSource]:
+    """Seeded illumination set (new; not in the reference): ``n_angles`` directions with (kx, ky) uniform in
+    the disk sin(theta) <= NA / n_bg, snapped to the lattice 2*pi*m/(N*dx) of the grid's x and y axes, each
+    with the polarisations named in ``polarizations`` ("s": k x z normalised, "p": s x k), both transverse
+    to k.  Returns the sources angle-major (s then p per angle)."""
+    rng = np.random.default_rng(seed + 1)
+    nbg = math.sqrt(permittivity_bg)
+    kbg = 2 * math.pi * nbg / wavelength
+    dk = [2 * math.pi / (grid_size[d] * resolution[d]) for d in range(2)]
+    ks = []
+    while len(ks) < n_angles:
+        r = math.sqrt(rng.uniform()) * na / nbg
+        phi = rng.uniform(0, 2 * math.pi)
+        kx, ky = kbg * r * math.cos(phi), kbg * r * math.sin(phi)
+        kx = round(kx / dk[0]) * dk[0]
+        ky = round(ky / dk[1]) * dk[1]
+        st = math.hypot(kx, ky) / kbg
+        if st > na / nbg:
+            continue
+        k = np.array([kx / kbg, ky / kbg, math.sqrt(max(0.0, 1 - st * st))])
+        ks.append(k / np.linalg.norm(k))
+    out = []
+    for k in ks:
+        s = np.cross(k, [0.0, 0.0, 1.0])
+        if np.linalg.norm(s) < 1e-12:
+            s = np.array([0.0, 1.0, 0.0])
+        s /= np.linalg.norm(s)
+        p = np.cross(s, k)
+        p /= np.linalg.norm(p)
+        for c in polarizations:
+            out.append(PlaneWaveSource(wavelength=wavelength, polarization=s if c == "s" else p, k_vector=k))
+    return out

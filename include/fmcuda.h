@@ -159,6 +159,32 @@ fm_status fm_copy_fields(fm_plan* plan, int nrhs, double* E_out, double* H_out);
 /* Wait for the plan's stream. */
 fm_status fm_synchronize(fm_plan* plan);
 
+/* ---- continuous batching: the slot engine ----------------------------------
+ * No counterpart in the reference (it solves one request per call).  An engine owns `slots` right-hand
+ * sides on one plan; each slot holds one plane-wave right-hand side on its own permittivity, with its own
+ * potential, eps_imag, Krylov basis of up to `basis` vectors and GMRES state (the reference's
+ * KrylovJL_GMRES semantics per right-hand side: warm start b, no restart, maxiters = max(2*Bornmax, 100)
+ * capped at `basis`, reltol = tolerance, abstol = tolerance*1e-2).  Requests share the engine's
+ * wavelength, background permittivity and attenuation filters (fx, fy, fz over the padded axes, NULL =
+ * ones) and take over the plan.  fm_engine_step admits queued right-hand sides into free slots, runs one
+ * Krylov iteration on every running slot in shared launches (slots at different iterations), and
+ * finishes the slots that stopped: their cropped total E and H are copied to the caller's host buffers
+ * given at submission (nrhs x (Nx,Ny,Nz,3) complex FP64 each), which must stay valid until then.
+ * fm_engine_submit may be called from another thread than fm_engine_step. */
+typedef struct fm_engine fm_engine;
+/* Device bytes one slot needs (basis vectors + work + outputs). */
+long long fm_engine_slot_bytes(const fm_plan_desc* desc, int basis);
+fm_status fm_engine_create(fm_plan* plan, int slots, int basis, double wavelength, double permittivity_bg,
+                           const double* fx, const double* fy, const double* fz, int ortho, fm_engine** out);
+void fm_engine_destroy(fm_engine* engine);
+fm_status fm_engine_submit(fm_engine* engine, long long request_id, const double* eps, int nrhs,
+                           const fm_plane_wave* sources, double tolerance, int iterations_max, double* E_out,
+                           double* H_out);
+/* Completed right-hand sides of this step: request id, index within the request and solve info. */
+fm_status fm_engine_step(fm_engine* engine, int* n_done, long long* done_request, int* done_rhs,
+                         fm_solve_info* done_info, int max_done);
+fm_status fm_engine_status(fm_engine* engine, int* running, int* queued);
+
 /* ---- Green application without device allocation ----------------------
  * No counterpart in the reference.  For callers that cannot let a library call cudaMalloc (their own
  * pooled allocator, a fixed device-memory budget, a loop that must not touch the allocator): the

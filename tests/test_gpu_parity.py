@@ -30,7 +30,8 @@ def _plan_with_oracle_potential(grid, bcs, precision):
 
 @pytest.mark.parametrize("precision", ["float64", "float32", "float32-math64"])
 @pytest.mark.parametrize("grid,kind", [((32, 32, 16), "absz"), ((16, 32, 8), "absz"), ((32, 16, 32), "per"),
-                                       ((64, 32, 32), "absz")])
+                                       ((64, 32, 32), "absz"), ((96, 32, 16), "absz"), ((32, 96, 16), "absz"),
+                                       ((16, 32, 96), "per")])
 def test_green_apply(precision, grid, kind):
     bcs = absorbing_z(grid[2]) if kind == "absz" else periodic()
     ocfg, solver, plan, pot = _plan_with_oracle_potential(grid, bcs, precision)
@@ -61,6 +62,14 @@ def test_curl(precision):
     E = random_field(ocfg.padded_size + (3,), 4)
     H = plan.curl_field(E)
     assert rel(H, O.magnetic_field(E, RES, WL)) < OP_TOL[precision]
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32-math64"])
+def test_solve_gmres_96_grid(precision):
+    """96-point x/y axes (radix 3) through the whole solve: the 96x96x64 serving grid shape at a smaller z."""
+    ref, out, solver = _solve_pair((96, 96, 8), 6.0, precision)
+    assert rel(out.E, ref.E) < SOLVE_TOL[precision]
+    assert rel(out.H, ref.H) < SOLVE_TOL[precision]
 
 
 def test_batched_operator_equals_single():
