@@ -197,7 +197,8 @@ def run(args):
     srcs = srcs[: args.nrhs]
     lists = [[s] for s in srcs]
     solver = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
-                                    precision=args.precision, linear_solver=F.KrylovJL_GMRES(ortho=args.ortho),
+                                    precision=args.precision,
+                                    linear_solver=F.KrylovJL_GMRES(ortho=args.ortho, block_size=args.block),
                                     max_rhs=args.nrhs, device_index=dev)
     plan = solver.plan()
     info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
@@ -315,7 +316,8 @@ def run(args):
                            "grid": list(GRID), "padded": list(solver.padded_size()), "rhs_per_gpu": args.nrhs,
                            "precision": f"{args.precision}: complex64 fields in HBM, FP64 dots"
                                         + (", FP64 FFT/Green/V arithmetic" if args.precision != "float32" else ""),
-                           "ortho": args.ortho, "parallelism": f"replicas{world}",
+                           "ortho": args.ortho + (f"-{args.block}" if args.ortho == "block" else ""),
+                           "parallelism": f"replicas{world}",
                            "l2": "inputs larger than L2 (Krylov basis of 50 MB vectors)", "seed": SEED},
                 "latency_s": {"p50": statistics.median(times), "p99": float(np.percentile(times, 99)),
                               "unit": "batched step"},
@@ -384,7 +386,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fmcuda", choices=["fmcuda", "reference"])
     ap.add_argument("--nrhs", type=int, default=64)
-    ap.add_argument("--ortho", default="cgs", choices=["mgs", "cgs", "cgs2"])
+    ap.add_argument("--ortho", default="cgs", choices=["mgs", "cgs", "cgs2", "block"])
+    ap.add_argument("--block", type=int, default=4, help="vectors per block for --ortho block")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=1)

@@ -97,7 +97,7 @@ struct fm_plan {
   DevBuf V;
   // workspace
   DevBuf t1, t2, bbuf, xbuf, ebuf, sbuf, basis, gbuf2;
-  DevBuf red_part, red_out, red_cnt, active, scale, coef, hbuf;
+  DevBuf red_part, red_out, red_cnt, active, scale, coef, hbuf, shifts, yblk, V64;
   DevBuf eps_dev, fx, fy, fz, maxpart, maxout;
   DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
   DevBuf Eo, Ho;
@@ -116,7 +116,7 @@ struct fm_plan {
 // kernel accounting
 // ---------------------------------------------------------------------------
 enum KCls { KC_XF = 0, KC_YF, KC_ZG, KC_YI, KC_XI, KC_DOT, KC_UPD, KC_MGS, KC_AXPBY, KC_CURL, KC_SETUP, KC_N };
-static const char* kcls_name[KC_N] = {"xf", "yf", "zg", "yi", "xi", "multidot", "update", "mgs", "axpby", "curl", "setup"};
+static const char* kcls_name[KC_N] = {"xf", "yf", "zg", "yi", "xi", "multidot", "update", "mgs/gram", "axpby", "curl", "setup"};
 
 static cudaEvent_t ev_get(fm_plan* P) {
   if (!P->evpool.empty()) {
@@ -729,6 +729,617 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
 }
 
 // ---------------------------------------------------------------------------
+// s-step (block) GMRES
+//
+// The stored basis is a sequence of raw vectors X_0..X_K-1 in U; the
+// orthonormal Arnoldi basis is V = X Rf^{-1}, with Rf upper triangular and
+// block diagonal (1x1 blocks for the classical Gram-Schmidt steps, S x S
+// blocks for each s-step block), held per RHS on the host in FP64.  Every
+// coefficient that touches the basis is transformed on the host, so the
+// device only sees raw combinations of stored vectors.
+//
+// After S classical Gram-Schmidt steps (which also give Ritz values for the
+// Newton shifts), each step from basis X_0..X_m (m = columns done):
+//   Y_0 = s0 X_m, Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}    (S operator applications)
+//   D = X^H Y, C = Rf^{-H} D (projection in V coordinates)   (one sweep of the basis)
+//   Y' = Y - X Rf^{-1} C, G = Y'^H Y'                        (one sweep of the basis)
+//   G = Rb^H Rb (Cholesky); X_{m+1..m+S} = Y', Rf block = Rb
+// and the Hessenberg columns m..m+S-1 follow from the relations
+//   (M^{-1}A) V W_{0:S-1} = V (W_{1:S} + W_{0:S-1} diag(theta)),
+// where W holds the V coordinates of Y_0..Y_S (block CA-GMRES change of
+// basis).  Givens rotations and the stopping test then run column by column,
+// as in gmres() above, so the iteration at which a RHS stops and the iterate
+// it returns are those of full GMRES (in exact arithmetic).
+// ---------------------------------------------------------------------------
+namespace {
+
+// eigenvalues of an n x n complex upper Hessenberg matrix (column-major), shifted QR with deflation
+bool hess_eigs(int n, std::vector<cd> A, std::vector<cd>& ev) {
+  ev.clear();
+  auto a = [&](int i, int j) -> cd& { return A[i + (size_t)j * n]; };
+  int hi = n - 1, iter = 0;
+  while (hi >= 0) {
+    if (hi == 0) {
+      ev.push_back(a(0, 0));
+      break;
+    }
+    int l = hi;
+    while (l > 0 && std::abs(a(l, l - 1)) > 1e-15 * (std::abs(a(l, l)) + std::abs(a(l - 1, l - 1)))) --l;
+    if (l == hi) {
+      ev.push_back(a(hi, hi));
+      --hi;
+      iter = 0;
+      continue;
+    }
+    if (++iter > 100 * n) return false;
+    // Wilkinson shift from the trailing 2x2 block of the window [l, hi]
+    const cd p = a(hi - 1, hi - 1), q = a(hi - 1, hi), r = a(hi, hi - 1), t = a(hi, hi);
+    const cd tr = p + t, det = p * t - q * r, disc = std::sqrt(tr * tr / 4.0 - det);
+    const cd m1 = tr / 2.0 + disc, m2 = tr / 2.0 - disc;
+    cd mu = std::abs(m1 - t) < std::abs(m2 - t) ? m1 : m2;
+    if (iter % 11 == 10) mu += std::abs(a(hi, hi - 1));  // exceptional shift
+    std::vector<double> cs(hi - l);
+    std::vector<cd> sn(hi - l);
+    for (int k = l; k <= hi; ++k) a(k, k) -= mu;
+    for (int k = l; k < hi; ++k) {  // A - mu I = Q R, Givens G_k zeroes a(k+1, k)
+      const cd x = a(k, k), y = a(k + 1, k);
+      const double nr = std::sqrt(std::norm(x) + std::norm(y));
+      double c = 1.0;
+      cd sg = 0.0;
+      if (nr > 0) {
+        c = std::abs(x) / nr;
+        sg = (std::abs(x) > 0 ? x / std::abs(x) : cd(1.0, 0.0)) * std::conj(y) / nr;
+      }
+      for (int j = k; j <= hi; ++j) {
+        const cd t1 = a(k, j), t2 = a(k + 1, j);
+        a(k, j) = c * t1 + sg * t2;
+        a(k + 1, j) = -std::conj(sg) * t1 + c * t2;
+      }
+      cs[k - l] = c;
+      sn[k - l] = sg;
+    }
+    for (int k = l; k < hi; ++k) {  // R Q = R G_l^H ... G_{hi-1}^H
+      const double c = cs[k - l];
+      const cd sg = sn[k - l];
+      for (int i = l; i <= k + 1; ++i) {
+        const cd t1 = a(i, k), t2 = a(i, k + 1);
+        a(i, k) = c * t1 + std::conj(sg) * t2;
+        a(i, k + 1) = -sg * t1 + c * t2;
+      }
+    }
+    for (int k = l; k <= hi; ++k) a(k, k) += mu;
+  }
+  return true;
+}
+
+// Leja ordering: start from the largest modulus, then maximise the product of distances
+void leja_order(std::vector<cd>& z) {
+  std::vector<cd> out;
+  std::vector<bool> used(z.size(), false);
+  for (size_t n = 0; n < z.size(); ++n) {
+    int best = -1;
+    double bv = -1.0;
+    for (size_t i = 0; i < z.size(); ++i) {
+      if (used[i]) continue;
+      double v = 1.0;
+      if (out.empty()) v = std::abs(z[i]);
+      else
+        for (const cd& o : out) v *= std::abs(z[i] - o);
+      if (v > bv) {
+        bv = v;
+        best = (int)i;
+      }
+    }
+    used[best] = true;
+    out.push_back(z[best]);
+  }
+  z = out;
+}
+
+// G = R^H R for an n x n Hermitian positive definite G (column-major); false when not positive definite
+bool chol_upper(int n, const std::vector<cd>& G, std::vector<cd>& R) {
+  R.assign((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    cd d = G[j + (size_t)j * n];
+    for (int k = 0; k < j; ++k) d -= std::conj(R[k + (size_t)j * n]) * R[k + (size_t)j * n];
+    if (!(d.real() > 0.0) || !std::isfinite(d.real())) return false;
+    const double rd = std::sqrt(d.real());
+    R[j + (size_t)j * n] = rd;
+    for (int i = j + 1; i < n; ++i) {
+      cd v = G[j + (size_t)i * n];
+      for (int k = 0; k < j; ++k) v -= std::conj(R[k + (size_t)j * n]) * R[k + (size_t)i * n];
+      R[j + (size_t)i * n] = v / rd;
+    }
+  }
+  return true;
+}
+
+struct BlkState {
+  bool active = true, solved = false;
+  double beta = 0, eps = 0, rnorm = 0;
+  int iters = 0;            // Krylov iterations (Hessenberg columns) taken
+  int nvec = 0;             // stored basis vectors
+  int ld = 0;               // leading dimension of H and Rf
+  std::vector<cd> H;        // V-coordinate Hessenberg, H[i + j*ld]
+  std::vector<cd> Rf;       // X = V Rf, Rf[i + k*ld]
+  std::vector<int> b0;      // first index of the diagonal block of Rf that holds column k
+  std::vector<double> c;    // Givens
+  std::vector<cd> s, z;
+  std::vector<std::vector<cd>> Rg;
+  std::vector<cd> theta;    // Newton shifts
+};
+
+// d = Rf^{-1} c over the first K indices (K ends on a block boundary)
+void rf_solve(const BlkState& st, int K, const cd* c, cd* d) {
+  for (int k = K - 1; k >= 0;) {
+    const int a0 = st.b0[k];
+    for (int i = k; i >= a0; --i) {
+      cd v = c[i];
+      for (int j = i + 1; j <= k; ++j) v -= st.Rf[i + (size_t)j * st.ld] * d[j];
+      d[i] = v / st.Rf[i + (size_t)i * st.ld];
+    }
+    k = a0 - 1;
+  }
+}
+
+// d = Rf^{-H} c over the first K indices
+void rf_solve_h(const BlkState& st, int K, const cd* c, cd* d) {
+  for (int k0 = 0; k0 < K;) {
+    int k1 = k0;
+    while (k1 + 1 < K && st.b0[k1 + 1] == k0) ++k1;
+    for (int i = k0; i <= k1; ++i) {
+      cd v = c[i];
+      for (int j = k0; j < i; ++j) v -= std::conj(st.Rf[j + (size_t)i * st.ld]) * d[j];
+      d[i] = v / std::conj(st.Rf[i + (size_t)i * st.ld]);
+    }
+    k0 = k1 + 1;
+  }
+}
+
+}  // namespace
+
+static int block_size_of(const fm_solve_opts& o) { return o.block > 0 ? o.block : 4; }
+
+template <typename R, typename YR, int S>
+static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, const void* Y, const int* act, int nact) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+  int nblk = 1;
+  size_t smem = 0;
+  if constexpr (S <= 4) {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
+        bps < 1)
+      bps = 1;
+    const long long maxb = (P->M + 127) / 128;
+    nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+  } else {
+    smem = blockdot_smem<R, TY>(K, S);
+    static bool attr = false;  // one instantiation per (R, TY, S): raise its dynamic shared memory limit once
+    if (!attr) {
+      cudaError_t ea = cudaFuncSetAttribute(k_blockdot<R, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)blockdot_smem<R, TY>(KV_KMAX, S));
+      if (ea != cudaSuccess) return ea;
+      attr = true;
+    }
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot<R, TY, S>, KV_THREADS, smem) != cudaSuccess ||
+        bps < 1)
+      bps = 1;
+    const long long maxb = (P->M + KB_TE - 1) / KB_TE;
+    nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+  }
+  cudaError_t e = P->red_part.ensure((size_t)nb * nblk * K * S * sizeof(double2));
+  if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
+  if (e != cudaSuccess) return e;
+  const double bytes = ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
+  if constexpr (S <= 4)
+    FM_TRACK(P, KC_DOT, bytes,
+             (k_blockdot_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+                 P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
+                 (unsigned*)P->red_cnt.p, act)));
+  else
+    FM_TRACK(P, KC_DOT, bytes,
+             (k_blockdot<R, TY, S><<<dim3(nblk, nb), KV_THREADS, smem, P->st>>>(
+                 P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
+                 (unsigned*)P->red_cnt.p, act)));
+  return cudaGetLastError();
+}
+
+template <typename R, typename YR, int S>
+static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, const void* Y, void* Z, const int* act,
+                                      int nact) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+  constexpr int NG = S * (S + 1) / 2;
+  const double bytes = ((double)(K + S) * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
+  if constexpr (S <= 4) {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S>, KV_THREADS, 0) !=
+            cudaSuccess ||
+        bps < 1)
+      bps = 1;
+    const long long maxb = (P->M + 32 * KV_WARPS - 1) / (32 * KV_WARPS);
+    const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+    FM_TRACK(P, KC_UPD, bytes,
+             (k_blockupdate_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+                 P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
+  } else {
+    int bps = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
+        bps < 1)
+      bps = 1;
+    const long long maxb = (P->M + KV_THREADS / KB_KS - 1) / (KV_THREADS / KB_KS);
+    const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+    FM_TRACK(P, KC_UPD, bytes,
+             (k_blockupdate<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+                 P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const int nblk_g = kv_blocks(P, k_blockgram<R, S>, nb);
+  e = P->red_part.ensure((size_t)nb * nblk_g * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
+  if (e != cudaSuccess) return e;
+  FM_TRACK(P, KC_MGS, (double)S * sizeof(T) * nact * P->M,
+           (k_blockgram<R, S><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, (const T*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
+  return cudaGetLastError();
+}
+
+template <typename R, typename YR>
+static cudaError_t block_kernels(fm_plan* P, bool dot, int S, int nb, int K, const void* U, const void* Y, void* Z,
+                                 const int* act, int nact) {
+  switch (S) {
+    case 2: return dot ? launch_blockdot<R, YR, 2>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 2>(P, nb, K, U, Y, Z, act, nact);
+    case 3: return dot ? launch_blockdot<R, YR, 3>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 3>(P, nb, K, U, Y, Z, act, nact);
+    case 4: return dot ? launch_blockdot<R, YR, 4>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 4>(P, nb, K, U, Y, Z, act, nact);
+    case 5: return dot ? launch_blockdot<R, YR, 5>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 5>(P, nb, K, U, Y, Z, act, nact);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// Block vectors are generated and kept in FP64 (YR = double) on FP64 and FP32-storage/FP64-arithmetic plans:
+// rounding the raw Krylov vectors to FP32 before they are orthogonalised is what costs accuracy in an s-step
+// basis.  The orthogonalised block is stored in the basis type.
+template <typename R, typename YR>
+static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info,
+                             double deadline) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+  const int S = block_size_of(o);
+  const size_t fe = (size_t)P->M;
+  const size_t fbytes = (size_t)nb * fe * sizeof(T);
+  const int itmax = std::max(1, o.maxiters);
+  const int cap = itmax + S + 1;  // stored vectors at most
+  if (cap > KV_KMAX) return fail(FM_ERR_UNSUPPORTED, "Krylov basis larger than 128 vectors");
+  if ((fe & 3) != 0) return fail(FM_ERR_UNSUPPORTED, "block Gram-Schmidt needs 3*N to be a multiple of 4");
+  FM_CK(P->basis.ensure((size_t)cap * fbytes));
+  FM_CK(P->scale.ensure((size_t)(KV_KMAX + 1) * nb * sizeof(double)));
+  FM_CK(P->active.ensure((size_t)nb * sizeof(int)));
+  FM_CK(P->coef.ensure((size_t)nb * KV_KMAX * 8 * sizeof(double2)));
+  FM_CK(P->shifts.ensure((size_t)nb * sizeof(double2)));
+  FM_CK(P->yblk.ensure((size_t)(S + 1) * nb * fe * sizeof(TY)));
+  FM_TRY(ensure_reduce(P, nb, KV_KMAX));
+  T* U = (T*)P->basis.p;
+  TY* Yb = (TY*)P->yblk.p;
+  // operator on the block vectors: FP64 potential when the block type is wider than the plan's storage
+  RhsCtx rcY;
+  rcY.V = P->V.p;
+  if (sizeof(TY) != sizeof(T)) {
+    FM_CK(P->V64.ensure((size_t)P->n * sizeof(double2)));
+    k_to_f64<R><<<2 * P->sms, 256, 0, P->st>>>(P->n, (const T*)P->V.p, 1.0, (double2*)P->V64.p);
+    FM_CK(cudaGetLastError());
+    rcY.V = P->V64.p;
+  }
+  double* sc = (double*)P->scale.p;
+  int* act = (int*)P->active.p;
+  const double btol = std::pow(2.220446049250313e-16, 0.75);
+  const int ld = cap + 1;
+
+  std::vector<BlkState> St(nb);
+  std::vector<int> acth(nb, 1);
+  EpiParams ep{};
+  ep.inv_eps = P->kref2 / P->eps_imag;
+  auto upload_active = [&]() -> fm_status {
+    FM_CK(cudaMemcpyAsync(act, acth.data(), nb * sizeof(int), cudaMemcpyHostToDevice, P->st));
+    return FM_OK;
+  };
+  auto count_active = [&]() {
+    int n = 0;
+    for (int b = 0; b < nb; ++b) n += acth[b];
+    return n;
+  };
+  // Givens update with Hessenberg column j of RHS r; true when the RHS stops at this column
+  auto givens_col = [&](BlkState& r, int j) -> bool {
+    const int K = j + 1;
+    std::vector<cd> col(K);
+    for (int i = 0; i < K; ++i) col[i] = r.H[i + (size_t)j * ld];
+    const double hb = r.H[(j + 1) + (size_t)j * ld].real();
+    for (int i = 0; i < K - 1; ++i) {
+      cd t = r.c[i] * col[i] + r.s[i] * col[i + 1];
+      col[i + 1] = std::conj(r.s[i]) * col[i] - r.c[i] * col[i + 1];
+      col[i] = t;
+    }
+    double c;
+    cd sn, rho;
+    sym_givens(col[K - 1], hb, c, sn, rho);
+    col[K - 1] = rho;
+    r.c.push_back(c);
+    r.s.push_back(sn);
+    r.Rg.push_back(col);
+    const cd zk1 = std::conj(sn) * r.z[K - 1];
+    r.z[K - 1] = c * r.z[K - 1];
+    r.rnorm = std::abs(zk1);
+    r.iters = K;
+    r.solved = (r.rnorm <= r.eps) || (r.rnorm + 1.0 <= 1.0);
+    if (r.solved || hb <= btol || K >= itmax) return true;
+    r.z.push_back(zk1);
+    return false;
+  };
+
+  // r0 = M^{-1}(b - A x) into X_0
+  FM_TRY(upload_active());
+  FM_TRY(green_op<R>(P, nb, P->xbuf.p, PRO_V, nullptr, EPI_PREC_RES, P->xbuf.p, P->bbuf.p, ep, U, act));
+  std::vector<double2> hv;
+  FM_TRY(multidot<R>(P, nb, 0, U, U, true, act, hv));
+  for (int b = 0; b < nb; ++b) {
+    BlkState& r = St[b];
+    r.ld = ld;
+    r.H.assign((size_t)ld * ld, 0.0);
+    r.Rf.assign((size_t)ld * ld, 0.0);
+    r.b0.assign(ld, 0);
+    r.beta = std::sqrt(hv[b].x);
+    r.rnorm = r.beta;
+    r.eps = o.abstol + o.reltol * r.beta;
+    info[b].residual0 = r.beta;
+    r.Rf[0] = r.beta;
+    r.b0[0] = 0;
+    r.nvec = 1;
+    r.z.assign(1, cd(r.beta, 0.0));
+    if (r.beta == 0.0 || r.rnorm <= r.eps) {
+      r.active = false;
+      r.solved = true;
+      acth[b] = 0;
+    }
+  }
+
+  // ---- phase 1: S classical Gram-Schmidt steps (Ritz values for the shifts) ----
+  int m = 0;  // columns done by the RHS still running
+  std::vector<double> sch(nb, 0.0);
+  while (count_active() > 0 && m < S && m < itmax) {
+    const int nact = count_active();
+    FM_TRY(upload_active());
+    for (int b = 0; b < nb; ++b) sch[b] = acth[b] ? 1.0 / St[b].Rf[m + (size_t)m * ld].real() : 0.0;
+    FM_CK(cudaMemcpyAsync(sc, sch.data(), nb * sizeof(double), cudaMemcpyHostToDevice, P->st));
+    T* Uj = U + (size_t)m * nb * fe;
+    T* Uw = U + (size_t)(m + 1) * nb * fe;
+    FM_TRY(green_op<R>(P, nb, Uj, PRO_V_SCALE, sc, EPI_PREC_OP, Uj, nullptr, ep, Uw, act, nact));
+    const int K = m + 1;
+    std::vector<double2> hr;
+    FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr, nact));
+    std::vector<double2> cf((size_t)nb * K, make_double2(0, 0));
+    for (int b = 0; b < nb; ++b) {
+      if (!acth[b]) continue;
+      for (int k = 0; k < K; ++k) {
+        const double rk = St[b].Rf[k + (size_t)k * ld].real();
+        const cd h = cd(hr[(size_t)b * K + k].x, hr[(size_t)b * K + k].y) / rk;
+        St[b].H[k + (size_t)m * ld] = h;
+        const cd e = h / rk;
+        cf[(size_t)b * K + k] = make_double2(e.real(), e.imag());
+      }
+    }
+    FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    Coef c{(const double2*)P->coef.p, K, nullptr, nb, -1.0, 0};
+    dim3 g(kv_blocks(P, k_update<R, true>, nb), nb);
+    FM_TRACK(P, KC_UPD, (double)(K + 2) * nact * fe * sizeof(T),
+             (k_update<R, true><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, K, U, c, Uw, nullptr, (double2*)P->red_part.p,
+                                                             (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
+    FM_CK(cudaGetLastError());
+    std::vector<double2> nn(nb);
+    FM_CK(cudaMemcpyAsync(nn.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+    tk_resolve(P);
+    for (int b = 0; b < nb; ++b) {
+      if (!acth[b]) continue;
+      BlkState& r = St[b];
+      const double hb = std::sqrt(std::max(0.0, nn[b].x));
+      r.H[(m + 1) + (size_t)m * ld] = hb;
+      r.Rf[(m + 1) + (size_t)(m + 1) * ld] = hb;
+      r.b0[m + 1] = m + 1;
+      r.nvec = m + 2;
+      if (givens_col(r, m)) {
+        r.active = false;
+        acth[b] = 0;
+      }
+    }
+    ++m;
+    if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
+  }
+  // Newton shifts: Ritz values of the leading S x S Hessenberg block, Leja ordered
+  for (int b = 0; b < nb; ++b) {
+    BlkState& r = St[b];
+    r.theta.assign(S, 0.0);
+    if (!r.active) continue;
+    std::vector<cd> Hs((size_t)S * S), ev;
+    for (int j = 0; j < S; ++j)
+      for (int i = 0; i < S; ++i) Hs[i + (size_t)j * S] = r.H[i + (size_t)j * ld];
+    if (hess_eigs(S, Hs, ev) && (int)ev.size() == S) {
+      leja_order(ev);
+      r.theta = ev;
+    }
+  }
+
+  // ---- phase 2: s-step blocks ----
+  while (count_active() > 0 && m < itmax) {
+    const int nact = count_active();
+    FM_TRY(upload_active());
+    const int K = m + 1;
+    // Y_0 = V_m = sum_k X_k (Rf^{-1})_{k,m} over m's diagonal block (the same block layout for every RHS)
+    int k0 = m;
+    for (int b = 0; b < nb; ++b)
+      if (acth[b]) k0 = St[b].b0[m];
+    const int nc = m - k0 + 1;
+    {
+      std::vector<double2> cc((size_t)nb * 8, make_double2(0, 0));
+      for (int b = 0; b < nb; ++b) {
+        if (!acth[b]) continue;
+        std::vector<cd> em(K, 0.0), d(K, 0.0);
+        em[m] = 1.0;
+        rf_solve(St[b], K, em.data(), d.data());
+        for (int a2 = 0; a2 < nc; ++a2) cc[(size_t)b * 8 + a2] = make_double2(d[k0 + a2].real(), d[k0 + a2].imag());
+      }
+      FM_CK(cudaMemcpyAsync(P->coef.p, cc.data(), cc.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+      FM_TRACK(P, KC_AXPBY, (double)nc * nact * fe * sizeof(T) + (double)nact * fe * sizeof(TY),
+               (k_combine<R, TY><<<dim3(2 * P->sms, nb), KV_THREADS, 0, P->st>>>(
+                   P->M, nb, k0, nc, U, (const double2*)P->coef.p, 8, Yb, act)));
+      FM_CK(cudaGetLastError());
+    }
+    // Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}, t = 1..S
+    std::vector<double2> th(nb);
+    for (int t = 1; t <= S; ++t) {
+      for (int b = 0; b < nb; ++b) th[b] = make_double2(St[b].theta[t - 1].real(), St[b].theta[t - 1].imag());
+      FM_CK(cudaMemcpyAsync(P->shifts.p, th.data(), nb * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+      EpiParams eps = ep;
+      eps.shift_b = (const double2*)P->shifts.p;
+      TY* Yin = Yb + (size_t)(t - 1) * nb * fe;
+      TY* Yout = Yb + (size_t)t * nb * fe;
+      // (the shift array is rewritten for the next vector in stream order, after this pass has read it)
+      FM_TRY(green_op<YR>(P, nb, Yin, PRO_V, nullptr, EPI_PREC_OP, Yin, nullptr, eps, Yout, act, nact, &rcY));
+    }
+    // D = X^H Y_{1..S}
+    FM_CK((block_kernels<R, YR>(P, true, S, nb, K, U, Yb + (size_t)nb * fe, nullptr, act, nact)));
+    std::vector<double2> D((size_t)nb * K * S);
+    FM_CK(cudaMemcpyAsync(D.data(), P->red_out.p, D.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+    tk_resolve(P);
+    // C = Rf^{-H} D (V coordinates), E = Rf^{-1} C (X coordinates) for the update
+    std::vector<std::vector<cd>> Cv(nb);
+    std::vector<double2> cf((size_t)nb * KV_KMAX * S, make_double2(0, 0));
+    for (int b = 0; b < nb; ++b) {
+      if (!acth[b]) continue;
+      Cv[b].assign((size_t)K * S, 0.0);
+      std::vector<cd> dcol(K), ccol(K), ecol(K);
+      for (int t = 0; t < S; ++t) {
+        for (int k = 0; k < K; ++k) {
+          const double2 v = D[((size_t)b * K + k) * S + t];
+          dcol[k] = cd(v.x, v.y);
+        }
+        rf_solve_h(St[b], K, dcol.data(), ccol.data());
+        rf_solve(St[b], K, ccol.data(), ecol.data());
+        for (int k = 0; k < K; ++k) {
+          Cv[b][k + (size_t)t * K] = ccol[k];
+          cf[(size_t)b * KV_KMAX * S + (size_t)k * S + t] = make_double2(ecol[k].real(), ecol[k].imag());
+        }
+      }
+    }
+    FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    // Y' = Y - X E into basis slots m+1..m+S, Gram of Y'
+    FM_CK((block_kernels<R, YR>(P, false, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
+    const int NG = S * (S + 1) / 2;
+    std::vector<double2> Gt((size_t)nb * NG);
+    FM_CK(cudaMemcpyAsync(Gt.data(), P->red_out.p, Gt.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+    FM_CK(cudaStreamSynchronize(P->st));
+    tk_resolve(P);
+    for (int b = 0; b < nb; ++b) {
+      if (!acth[b]) continue;
+      BlkState& r = St[b];
+      std::vector<cd> G((size_t)S * S), Rb;
+      int gi = 0;
+      for (int t = 0; t < S; ++t)
+        for (int u = t; u < S; ++u, ++gi) {
+          const cd v(Gt[(size_t)b * NG + gi].x, Gt[(size_t)b * NG + gi].y);
+          G[t + (size_t)u * S] = v;
+          G[u + (size_t)t * S] = std::conj(v);
+        }
+      if (!chol_upper(S, G, Rb)) {  // the block lost rank: Krylov breakdown, keep the columns so far
+        r.active = false;
+        acth[b] = 0;
+        continue;
+      }
+      for (int u = 0; u < S; ++u) {
+        for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = Rb[a + (size_t)u * S];
+        r.b0[K + u] = K;
+      }
+      r.nvec = K + S;
+      // W: V coordinates of Y_0..Y_S, n x (S+1)
+      const int n = K + S;
+      std::vector<cd> W((size_t)n * (S + 1), 0.0);
+      W[m] = 1.0;  // Y_0 = V_m
+      for (int t = 0; t < S; ++t) {
+        for (int i = 0; i < K; ++i) W[i + (size_t)(t + 1) * n] = Cv[b][i + (size_t)t * K];
+        for (int a = 0; a < S; ++a) W[K + a + (size_t)(t + 1) * n] = Rb[a + (size_t)t * S];
+      }
+      // Rh = W[:,1:S] + W[:,0:S-1] diag(theta) - [H_{0:m,0:m-1} W_{0:m-1,0:S-1}; 0]
+      std::vector<cd> Rh((size_t)n * S), Hn((size_t)n * S);
+      for (int c = 0; c < S; ++c) {
+        for (int i = 0; i < n; ++i) Rh[i + (size_t)c * n] = W[i + (size_t)(c + 1) * n] + r.theta[c] * W[i + (size_t)c * n];
+        for (int j = 0; j < m; ++j) {
+          const cd w = W[j + (size_t)c * n];
+          if (w == cd(0.0, 0.0)) continue;
+          for (int i = 0; i <= j + 1; ++i) Rh[i + (size_t)c * n] -= r.H[i + (size_t)j * ld] * w;
+        }
+      }
+      // Hn = Rh T^{-1}, T = W[m..m+S-1, 0..S-1] upper triangular
+      for (int c = 0; c < S; ++c)
+        for (int i = 0; i < n; ++i) {
+          cd v = Rh[i + (size_t)c * n];
+          for (int a = 0; a < c; ++a) v -= Hn[i + (size_t)a * n] * W[m + a + (size_t)c * n];
+          Hn[i + (size_t)c * n] = v / W[m + c + (size_t)c * n];
+        }
+      for (int c = 0; c < S; ++c)
+        for (int i = 0; i < n; ++i) r.H[i + (size_t)(m + c) * ld] = (i <= m + c + 1) ? Hn[i + (size_t)c * n] : cd(0.0, 0.0);
+      for (int c = 0; c < S; ++c) {
+        if (givens_col(r, m + c)) {
+          r.active = false;
+          acth[b] = 0;
+          break;
+        }
+      }
+    }
+    m += S;
+    if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
+  }
+
+  // ---- x += V y = X Rf^{-1} y ----
+  std::vector<double2> yh((size_t)nb * KV_KMAX, make_double2(0, 0));
+  int Kmax = 0;
+  for (int b = 0; b < nb; ++b) {
+    BlkState& r = St[b];
+    const int n_in = r.iters;
+    if (n_in == 0) continue;
+    std::vector<cd> y(r.z.begin(), r.z.begin() + n_in);
+    for (int i = n_in - 1; i >= 0; --i) {
+      for (int jj = n_in - 1; jj > i; --jj) y[i] -= r.Rg[jj][i] * y[jj];
+      if (std::abs(r.Rg[i][i]) <= btol) {
+        for (int q = 0; q <= i; ++q) y[q] = 0.0;
+        break;
+      }
+      y[i] /= r.Rg[i][i];
+    }
+    std::vector<cd> yv(r.nvec, 0.0), d(r.nvec, 0.0);
+    for (int i = 0; i < n_in; ++i) yv[i] = y[i];
+    rf_solve(r, r.nvec, yv.data(), d.data());
+    for (int i = 0; i < r.nvec; ++i) yh[(size_t)b * KV_KMAX + i] = make_double2(d[i].real(), d[i].imag());
+    Kmax = std::max(Kmax, r.nvec);
+  }
+  if (Kmax > 0) {
+    FM_CK(cudaMemcpyAsync(P->coef.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    Coef cf{(const double2*)P->coef.p, KV_KMAX, nullptr, nb, 1.0, 1};
+    dim3 g(kv_blocks(P, k_update<R, false>, nb), nb);
+    FM_TRACK(P, KC_UPD, (double)(Kmax + 2) * nb * fe * sizeof(T),
+             (k_update<R, false><<<g, KV_THREADS, 0, P->st>>>(P->M, nb, Kmax, U, cf, (T*)P->xbuf.p, nullptr, nullptr,
+                                                              nullptr, nullptr, nullptr)));
+    FM_CK(cudaGetLastError());
+  }
+  for (int b = 0; b < nb; ++b) {
+    info[b].iterations = St[b].iters;
+    info[b].solved = St[b].solved ? 1 : 0;
+    info[b].residual = St[b].rnorm;
+  }
+  return FM_OK;
+}
+
+// ---------------------------------------------------------------------------
 // BiCGStab (left preconditioned, Krylov.jl form, shadow c = b) and the plain
 // Born series (Richardson) on the same operator.
 // ---------------------------------------------------------------------------
@@ -941,7 +1552,10 @@ static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
   FM_TRY(green_op<R>(P, nb, P->sbuf.p, PRO_COPY, nullptr, EPI_STORE, nullptr, nullptr, ep, P->bbuf.p, nullptr));
   FM_CK(cudaMemcpyAsync(P->xbuf.p, P->bbuf.p, fbytes, cudaMemcpyDeviceToDevice, P->st));
   fm_status st;
-  if (o.method == FM_METHOD_GMRES) st = gmres<R>(P, nb, o, info, deadline);
+  if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK)
+    st = P->prec == FM_PREC_F32 ? gmres_block<R, R>(P, nb, o, info, deadline)
+                                : gmres_block<R, double>(P, nb, o, info, deadline);
+  else if (o.method == FM_METHOD_GMRES) st = gmres<R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_BICGSTAB) st = bicgstab<R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_RICHARDSON) st = richardson<R>(P, nb, o, info, deadline);
   else return fail(FM_ERR_INVALID, "unknown method");
@@ -986,7 +1600,13 @@ static fm_status validate_opts(const fm_solve_opts* o) {
   if (!(o->reltol >= 0 && o->reltol <= 1)) return fail(FM_ERR_INVALID, "tolerance must be in [0, 1]");
   if (!(o->abstol >= 0)) return fail(FM_ERR_INVALID, "abstol must be >= 0");
   if (o->method < 0 || o->method > 2) return fail(FM_ERR_INVALID, "unknown method");
-  if (o->ortho < 0 || o->ortho > 2) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
+  if (o->ortho < 0 || o->ortho > 3) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
+  if (o->ortho == FM_ORTHO_BLOCK && o->method == FM_METHOD_GMRES) {
+    if (o->block != 0 && (o->block < 2 || o->block > 5)) return fail(FM_ERR_INVALID, "block size must be 2..5");
+    if (o->restart > 0) return fail(FM_ERR_UNSUPPORTED, "block GMRES runs full GMRES only (restart = 0)");
+    if (o->maxiters + block_size_of(*o) + 1 > KV_KMAX)
+      return fail(FM_ERR_UNSUPPORTED, "GMRES basis larger than 128 vectors");
+  }
   if (o->restart < 0) return fail(FM_ERR_INVALID, "restart must be >= 0");
   if (o->method == FM_METHOD_GMRES) {
     const int mem = o->restart > 0 ? std::min(o->restart, o->maxiters) : o->maxiters;
@@ -1002,12 +1622,17 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   const size_t fb = (size_t)P->M * sizeof(cplx<R>);
   int vecs = 0;
   if (o.method == FM_METHOD_GMRES) vecs = (o.restart > 0 ? std::min(o.restart, o.maxiters) : o.maxiters) + 1;
+  size_t extra = 0;  // block GMRES: FP64 block vectors, FP64 pass temporaries, FP64 potential
+  if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK) {
+    vecs = o.maxiters + block_size_of(o) + 1;
+    extra = (size_t)P->M * sizeof(double2) * (block_size_of(o) + 1 + 2);
+  }
   else if (o.method == FM_METHOD_BICGSTAB) vecs = 6;
   else vecs = 1;
   // basis + b + x + s + e + t1 + t2 + fp64 staging and outputs
-  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 3;
+  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 3 + extra;
   const size_t held = P->basis.cap + P->bbuf.cap + P->xbuf.cap + P->sbuf.cap + P->ebuf.cap + P->t1.cap + P->t2.cap +
-                      P->gbuf2.cap + P->Eo.cap + P->Ho.cap;
+                      P->gbuf2.cap + P->Eo.cap + P->Ho.cap + P->yblk.cap;
   const size_t avail = (size_t)((freeb + held) * 0.92);
   wave = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, avail / per));
   wave = std::min(wave, std::max(1, P->desc.max_rhs));

@@ -284,6 +284,452 @@ __global__ void __launch_bounds__(KV_THREADS) k_mgs(long long M, int B, int i, i
   }
 }
 
+// ---------------------------------------------------------------------------
+// Block (s-step) Gram-Schmidt kernels.  The basis of RHS b is the sequence of
+// stored vectors X_k = U[(k*B + b)*M], k < K; the S block vectors are
+// Y_t = Y[(t*B + b)*M] in their own buffer and type TY (complex FP64 or the
+// basis type).  M must be a multiple of 4.
+// ---------------------------------------------------------------------------
+
+// out[b] = sum_{a<n} c[b*cs + a] * X_{k0+a}[b]   (FP64 accumulation)
+template <typename R, typename TY>
+__global__ void __launch_bounds__(KV_THREADS) k_combine(long long M, int B, int k0, int n, const cplx<R>* __restrict__ U,
+                                                        const double2* __restrict__ c, int cs, TY* __restrict__ out,
+                                                        const int* __restrict__ active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  __shared__ double2 cc[8];
+  if (threadIdx.x < n) cc[threadIdx.x] = c[(size_t)b * cs + threadIdx.x];
+  __syncthreads();
+  TY* ob = out + (size_t)b * M;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < M; e += (long long)gridDim.x * blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int a = 0; a < n; ++a) {
+      const double2 x = to_d(U[((size_t)(k0 + a) * B + b) * M + e]);
+      acc.x = fma(cc[a].x, x.x, fma(-cc[a].y, x.y, acc.x));
+      acc.y = fma(cc[a].x, x.y, fma(cc[a].y, x.x, acc.y));
+    }
+    ob[e] = from_d<TY>(acc);
+  }
+}
+// Block dot tiles hold the basis values widened to complex FP64 (16 bytes each): KB_TE values per row,
+// value c of row k stored at position c ^ (k & 7), so eight lanes reading the same column of eight
+// consecutive rows hit eight different 16-byte bank groups.  Each basis value is widened once, when it
+// is staged; the inner loop only reads FP64 values.
+constexpr int KB_TE = 32;
+constexpr int KB_PF = KV_KMAX * KB_TE / KV_THREADS;  // staged values per thread and tile, at most
+
+template <typename R, typename TY>
+__host__ __device__ constexpr size_t blockdot_smem(int K, int S) {
+  return (size_t)K * KB_TE * sizeof(double2) + (size_t)S * KB_TE * sizeof(double2) >
+                 (size_t)KV_THREADS * S * sizeof(double2)
+             ? (size_t)K * KB_TE * sizeof(double2) + (size_t)S * KB_TE * sizeof(double2)
+             : (size_t)KV_THREADS * S * sizeof(double2);
+}
+
+// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 accumulation, deterministic)
+// The block streams its element range in tiles of KB_TE elements of the K basis vectors and the S block
+// vectors.  The next tile is loaded into registers while this one is used from shared memory; each
+// thread owns one basis vector k (and a share of the tile's elements) and keeps its S dot products in
+// registers across all tiles: no per-tile cross-lane reduction.
+template <typename R, typename TY, int S>
+__global__ void __launch_bounds__(KV_THREADS) k_blockdot(long long M, int B, int K, const cplx<R>* __restrict__ U,
+                                                         const TY* __restrict__ Y, double2* __restrict__ part,
+                                                         double2* __restrict__ out, unsigned* __restrict__ counter,
+                                                         const int* __restrict__ active) {
+  using T = cplx<R>;
+  extern __shared__ __align__(16) unsigned char kb_smem[];
+  double2* Xs = reinterpret_cast<double2*>(kb_smem);   // [K][KB_TE], swizzled
+  double2* Ys = Xs + (size_t)K * KB_TE;                 // [S][KB_TE]
+  const int b = blockIdx.y, nblk = gridDim.x;
+  if (active && !active[b]) return;
+  const int Kp = (K + 31) & ~31;
+  const int G = KV_THREADS / Kp;
+  const int k = threadIdx.x % Kp, pr = threadIdx.x / Kp;
+  double2 acc[S];
+#pragma unroll
+  for (int t = 0; t < S; ++t) acc[t] = make_double2(0.0, 0.0);
+  const long long per = ((M + nblk - 1) / nblk + KB_TE - 1) / KB_TE * KB_TE;
+  const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
+  const size_t us = (size_t)B * M;
+  // staging: thread copies column sc = tid % KB_TE of rows sr, sr + 8, ...
+  const int sc = threadIdx.x % KB_TE, sr = threadIdx.x / KB_TE;
+  constexpr int RS = KV_THREADS / KB_TE;  // rows per staging pass
+  const T* xsrc = U + (size_t)b * M + (size_t)sr * us + sc;
+  const TY* ysrc = Y + (size_t)b * M;
+  T xr[KB_PF];
+  TY yr = TY{};
+  auto load = [&](long long e0) {
+    const bool v = e0 + sc < hi;
+#pragma unroll
+    for (int j = 0; j < KB_PF; ++j) {
+      xr[j].x = 0;
+      xr[j].y = 0;
+      if (v && sr + j * RS < K) xr[j] = xsrc[e0 + (size_t)j * RS * us];
+    }
+    if (threadIdx.x < S * KB_TE) {
+      const int t = threadIdx.x / KB_TE;
+      yr.x = 0;
+      yr.y = 0;
+      if (v) yr = ysrc[t * us + e0 + sc];
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int j = 0; j < KB_PF; ++j) {
+      const int kk = sr + j * RS;
+      if (kk < K) Xs[kk * KB_TE + (sc ^ (kk & 7))] = to_d(xr[j]);
+    }
+    if (threadIdx.x < S * KB_TE) Ys[threadIdx.x] = to_d(yr);
+  };
+  if (lo < hi) load(lo);
+  for (long long e0 = lo; e0 < hi; e0 += KB_TE) {
+    __syncthreads();  // the previous tile has been used
+    store();
+    __syncthreads();
+    if (e0 + KB_TE < hi) load(e0 + KB_TE);  // in flight while this tile is used
+    if (k < K) {
+      const double2* row = Xs + (size_t)k * KB_TE;
+      for (int c = pr; c < KB_TE; c += G) {
+        const double2 u = row[c ^ (k & 7)];
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          const double2 y = Ys[t * KB_TE + c];
+          acc[t].x = fma(u.x, y.x, fma(u.y, y.y, acc[t].x));
+          acc[t].y = fma(u.x, y.y, fma(-u.y, y.x, acc[t].y));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  double2* red = reinterpret_cast<double2*>(kb_smem);  // [KV_THREADS][S]
+#pragma unroll
+  for (int t = 0; t < S; ++t) red[threadIdx.x * S + t] = acc[t];
+  __syncthreads();
+  const int KS = K * S;
+  for (int o = threadIdx.x; o < KS; o += blockDim.x) {
+    const int kk = o / S, t = o - kk * S;
+    double2 sum = make_double2(0.0, 0.0);
+    for (int q = 0; q < G; ++q) {
+      const double2 v = red[(q * Kp + kk) * S + t];
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    part[((size_t)b * nblk + blockIdx.x) * KS + o] = sum;
+  }
+  finish_reduce(part, out, counter, KS, nblk, b);
+}
+
+// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  for t < S (FP64 accumulation; Z_t stored in the basis
+// type at Z[(t*B + b)*M]).  KB_KS threads share each element, thread q summing the basis vectors
+// k = q, q + KB_KS, ...: short dependency chains and KB_KS times more elements in flight per register.
+// The partial sums meet in shared memory.
+constexpr int KB_KS = 4;
+template <typename R, typename TY, int S>
+__global__ void __launch_bounds__(KV_THREADS) k_blockupdate(long long M, int B, int K, const cplx<R>* U, const TY* Y,
+                                                            cplx<R>* Z, const double2* __restrict__ coef,
+                                                            const int* __restrict__ active) {
+  using T = cplx<R>;
+  constexpr int NE = KV_THREADS / KB_KS;  // elements per block round
+  constexpr int KU = 4;                   // loads in flight per thread
+  __shared__ double2 cs[KV_KMAX * S];
+  __shared__ double2 red[KB_KS - 1][S][NE];
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  for (int i = threadIdx.x; i < K * S; i += blockDim.x) cs[i] = coef[(size_t)b * KV_KMAX * S + i];
+  __syncthreads();
+  const int el = threadIdx.x % NE, q = threadIdx.x / NE;
+  const TY* yb = Y + (size_t)b * M;
+  T* zb = Z + (size_t)b * M;
+  const size_t us = (size_t)B * M;
+  const T* ub = U + (size_t)b * M + (size_t)q * us;
+  const long long rounds = (M + NE - 1) / NE;
+  for (long long r = blockIdx.x; r < rounds; r += gridDim.x) {
+    const long long e = r * NE + el;
+    const bool in = e < M;
+    double2 acc[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) acc[t] = make_double2(0.0, 0.0);
+    const T* xp = ub + e;
+    for (int k = q; k < K; k += KB_KS * KU) {
+      T xr[KU];
+#pragma unroll
+      for (int u = 0; u < KU; ++u) {
+        xr[u].x = 0;
+        xr[u].y = 0;
+        if (in && k + u * KB_KS < K) xr[u] = xp[(size_t)(k - q + u * KB_KS) * us];
+      }
+#pragma unroll
+      for (int u = 0; u < KU; ++u) {
+        const int kk = k + u * KB_KS;
+        if (kk >= K) break;
+        const double2 x = to_d(xr[u]);
+#pragma unroll
+        for (int t = 0; t < S; ++t) {
+          const double2 c = cs[kk * S + t];
+          acc[t].x = fma(c.x, x.x, fma(-c.y, x.y, acc[t].x));
+          acc[t].y = fma(c.x, x.y, fma(c.y, x.x, acc[t].y));
+        }
+      }
+    }
+    if (q > 0) {
+#pragma unroll
+      for (int t = 0; t < S; ++t) red[q - 1][t][el] = acc[t];
+    }
+    __syncthreads();
+    if (q == 0 && in) {
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        double2 v = to_d(yb[t * us + e]);
+        v.x -= acc[t].x;
+        v.y -= acc[t].y;
+#pragma unroll
+        for (int qq = 0; qq < KB_KS - 1; ++qq) {
+          v.x -= red[qq][t][el].x;
+          v.y -= red[qq][t][el].y;
+        }
+        zb[t * us + e] = from_d<T>(v);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core (mma.sync m8n8k4 .f64) forms of the block dot and block
+// update, for S <= 4 block vectors.  The real and imaginary parts of the S
+// block vectors (or coefficients) fill the 8 columns of the B operand (columns
+// t: real part of vector t, 4 + t: imaginary part; columns of t >= S are zero),
+// and the real and imaginary parts of the basis values are the A operands of two
+// MMAs, P and Q, so that for column t
+//   conj(x) y:  Re = P[t] + Q[4+t],   Im = P[4+t] - Q[t]
+//   x c:        Re = P[t] - Q[4+t],   Im = P[4+t] + Q[t].
+// Fragment layout of m8n8k4 (row.col): A[gid][tig], B[tig][gid] and
+// C[gid][2 tig + i] for lane = 4 gid + tig.  Each lane reads a run of four
+// consecutive elements (32 bytes of complex FP32); the summed element index is
+// permuted in the same way for both operands, which leaves the products as they are.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 4)
+template <typename R, typename TY, int S>
+__global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B, int K, const cplx<R>* __restrict__ U,
+                                                             const TY* __restrict__ Y, double2* __restrict__ part,
+                                                             double2* __restrict__ out, unsigned* __restrict__ counter,
+                                                             const int* __restrict__ active) {
+  static_assert(S <= 4, "block dot on tensor cores takes at most 4 block vectors");
+  using T = cplx<R>;
+  constexpr int GPW = 4;  // groups of 8 basis vectors per warp
+  __shared__ double2 red[KV_WARPS][GPW * 8][S];
+  const int b = blockIdx.y, nblk = gridDim.x;
+  if (active && !active[b]) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const int KG = (K + 7) >> 3, KW = (KG + GPW - 1) / GPW, EW = KV_WARPS / KW;
+  const int kw = w % KW, ew = w / KW;
+  double P[GPW][2], Q[GPW][2];
+#pragma unroll
+  for (int g = 0; g < GPW; ++g) P[g][0] = P[g][1] = Q[g][0] = Q[g][1] = 0.0;
+  const long long per = ((M + nblk - 1) / nblk + 15) / 16 * 16;
+  const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
+  const size_t us = (size_t)B * M;
+  const T* ub = U + (size_t)b * M;
+  const TY* yb = Y + (size_t)b * M;
+  const int yt = gid & 3;                   // block vector of this lane's B column
+  const bool yim = gid >= 4, yon = yt < S;  // imaginary part / column in use
+  if (ew < EW) {
+    for (long long e0 = lo + (long long)ew * 16; e0 < hi; e0 += (long long)EW * 16) {
+      const long long eb = e0 + 4 * tig;  // this lane's run of 4 elements (wholly inside or outside)
+      const bool ein = eb < hi;
+      double bf[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        bf[q] = 0.0;
+        if (yon && ein) {
+          const double2 y = to_d(yb[yt * us + eb + q]);
+          bf[q] = yim ? y.y : y.x;
+        }
+      }
+#pragma unroll
+      for (int g = 0; g < GPW; ++g) {
+        if ((kw * GPW + g) >= KG) break;  // warp-uniform
+        const int k = (kw * GPW + g) * 8 + gid;
+        T xv[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          xv[q].x = 0;
+          xv[q].y = 0;
+        }
+        if (k < K && ein) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) xv[q] = ub[(size_t)k * us + eb + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 x = to_d(xv[q]);
+          mma_f64(P[g][0], P[g][1], x.x, bf[q]);
+          mma_f64(Q[g][0], Q[g][1], x.y, bf[q]);
+        }
+      }
+    }
+  }
+  // columns 2 tig, 2 tig + 1 of P and Q; the partner lane tig ^ 2 holds columns 4 + (2 tig, 2 tig + 1)
+#pragma unroll
+  for (int g = 0; g < GPW; ++g) {
+    const double pp0 = __shfl_xor_sync(0xffffffffu, P[g][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[g][1], 2);
+    const double qp0 = __shfl_xor_sync(0xffffffffu, Q[g][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[g][1], 2);
+    if (tig < 2) {
+      const int t0 = 2 * tig;
+      if (t0 < S) red[w][g * 8 + gid][t0] = make_double2(P[g][0] + qp0, pp0 - Q[g][0]);
+      if (t0 + 1 < S) red[w][g * 8 + gid][t0 + 1] = make_double2(P[g][1] + qp1, pp1 - Q[g][1]);
+    }
+  }
+  __syncthreads();
+  const int KS = K * S;
+  for (int o = threadIdx.x; o < KS; o += blockDim.x) {
+    const int k = o / S, t = o - k * S;
+    const int kg = k >> 3, kwo = kg / GPW, g = kg - kwo * GPW;
+    double2 sum = make_double2(0.0, 0.0);
+    for (int e = 0; e < EW; ++e) {
+      const double2 v = red[e * KW + kwo][g * 8 + (k & 7)][t];
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    part[((size_t)b * nblk + blockIdx.x) * KS + o] = sum;
+  }
+  finish_reduce(part, out, counter, KS, nblk, b);
+}
+
+// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 4).  A warp owns 32
+// elements (lane gid: elements 4 gid .. 4 gid + 3 of the tile) and runs over the basis 4 vectors at a time.
+template <typename R, typename TY, int S>
+__global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
+                                                                const TY* Y, cplx<R>* Z,
+                                                                const double2* __restrict__ coef,
+                                                                const int* __restrict__ active) {
+  static_assert(S <= 4, "block update on tensor cores takes at most 4 block vectors");
+  using T = cplx<R>;
+  __shared__ double Bs[KV_KMAX][8];  // B[k][col]: col t = Re E[k][t], 4 + t = Im E[k][t]
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  for (int i = threadIdx.x; i < KV_KMAX * 8; i += blockDim.x) {
+    const int k = i >> 3, col = i & 7, t = col & 3;
+    double v = 0.0;
+    if (k < K && t < S) {
+      const double2 c = coef[(size_t)b * KV_KMAX * S + k * S + t];
+      v = col >= 4 ? c.y : c.x;
+    }
+    Bs[k][col] = v;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  const size_t us = (size_t)B * M;
+  const T* ub = U + (size_t)b * M;
+  const TY* yb = Y + (size_t)b * M;
+  T* zb = Z + (size_t)b * M;
+  const long long tiles = (M + 31) / 32;
+  for (long long tl = (long long)blockIdx.x * KV_WARPS + w; tl < tiles; tl += (long long)gridDim.x * KV_WARPS) {
+    const long long ea = tl * 32 + 4 * gid;  // A rows of this lane: elements ea .. ea + 3 (wholly in or out)
+    const bool ein = ea < M;
+    double P[4][2], Q[4][2];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) P[q][0] = P[q][1] = Q[q][0] = Q[q][1] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += 4) {
+      const int k = k0 + tig;
+      T xv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        xv[q].x = 0;
+        xv[q].y = 0;
+      }
+      if (k < K && ein) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) xv[q] = ub[(size_t)k * us + ea + q];
+      }
+      const double bfr = Bs[k0 + tig][gid];  // rows past K are zero
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double2 x = to_d(xv[q]);
+        mma_f64(P[q][0], P[q][1], x.x, bfr);
+        mma_f64(Q[q][0], Q[q][1], x.y, bfr);
+      }
+    }
+    // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double pp0 = __shfl_xor_sync(0xffffffffu, P[q][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[q][1], 2);
+      const double qp0 = __shfl_xor_sync(0xffffffffu, Q[q][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[q][1], 2);
+      // C row gid is element tl*32 + 4*gid + q, i.e. this lane's own A row q
+      const long long e = ea + q;
+      if (tig < 2 && ein) {
+        const int t0 = 2 * tig;
+        if (t0 < S) {
+          const double2 y = to_d(yb[t0 * us + e]);
+          zb[t0 * us + e] = from_d<T>(make_double2(y.x - (P[q][0] - qp0), y.y - (pp0 + Q[q][0])));
+        }
+        if (t0 + 1 < S) {
+          const double2 y = to_d(yb[(t0 + 1) * us + e]);
+          zb[(t0 + 1) * us + e] = from_d<T>(make_double2(y.x - (P[q][1] - qp1), y.y - (pp1 + Q[q][1])));
+        }
+      }
+    }
+  }
+}
+
+// Gram matrix of S stored vectors Z_t = Z[(t*B + b)*M]:  out[b][tri(t,u)] = <Z_t, Z_u>, t <= u,
+// tri(t,u) = t*S - t*(t-1)/2 + (u-t)   (FP64 accumulation, deterministic).
+template <typename R, int S>
+__global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, const cplx<R>* __restrict__ Z,
+                                                          double2* __restrict__ part, double2* __restrict__ out,
+                                                          unsigned* __restrict__ counter,
+                                                          const int* __restrict__ active) {
+  constexpr int NG = S * (S + 1) / 2;
+  __shared__ double2 red[KV_WARPS][NG];
+  const int b = blockIdx.y, nblk = gridDim.x;
+  if (active && !active[b]) return;
+  double2 gram[NG];
+#pragma unroll
+  for (int i = 0; i < NG; ++i) gram[i] = make_double2(0.0, 0.0);
+  const cplx<R>* zb = Z + (size_t)b * M;
+  const size_t us = (size_t)B * M;
+  const long long per = (M + nblk - 1) / nblk;
+  const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
+  for (long long e = lo + threadIdx.x; e < hi; e += blockDim.x) {
+    double2 st[S];
+#pragma unroll
+    for (int t = 0; t < S; ++t) st[t] = to_d(zb[t * us + e]);
+    int gi = 0;
+#pragma unroll
+    for (int t = 0; t < S; ++t)
+#pragma unroll
+      for (int u = t; u < S; ++u, ++gi) {
+        gram[gi].x = fma(st[t].x, st[u].x, fma(st[t].y, st[u].y, gram[gi].x));
+        gram[gi].y = fma(st[t].x, st[u].y, fma(-st[t].y, st[u].x, gram[gi].y));
+      }
+  }
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NG; ++i) {
+    const double2 v = warp_sum(gram[i]);
+    if (lane == 0) red[wi][i] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < NG; i += blockDim.x) {
+    double2 sum = make_double2(0.0, 0.0);
+    for (int q = 0; q < KV_WARPS; ++q) {
+      sum.x += red[q][i].x;
+      sum.y += red[q][i].y;
+    }
+    part[((size_t)b * nblk + blockIdx.x) * NG + i] = sum;
+  }
+  finish_reduce(part, out, counter, NG, nblk, b);
+}
+
 // Generic batched elementwise combination (FP64 arithmetic):
 //   y[b] = ca[b]*a[b] + cb[b]*bv[b] + cc[b]*c[b]     (missing operands are skipped)
 // coefficients are complex per RHS.  Optionally reduces ||y||^2 into out[b].

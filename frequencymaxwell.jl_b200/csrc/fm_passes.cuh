@@ -329,6 +329,7 @@ struct EpiParams {
   double alpha_re, alpha_im, beta_re, beta_im;
   double inv_eps;  // 1/eps_imag (scaled units)
   const double* inv_eps_b = nullptr;  // per-RHS 1/eps_imag (null: inv_eps for all)
+  const double2* shift_b = nullptr;   // EPI_PREC_OP: per-RHS shift theta, out = M^{-1}A x - theta x
 };
 
 template <typename S, typename R, int L, int EPI>
@@ -395,6 +396,7 @@ __global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ 
       } else if constexpr (EPI == EPI_PREC_OP) {
         T xx = cscale(cv<T>(xvb[ix]), s);
         r = cmul(gam[e], csub(xx, g));
+        if (ep.shift_b) r = csub(r, cmul(mk((R)ep.shift_b[b].x, (R)ep.shift_b[b].y), xx));
       } else {
         T xx = cscale(cv<T>(xvb[ix]), s);
         r = cmul(gam[e], cadd(csub(cv<T>(bvb[ix]), xx), g));

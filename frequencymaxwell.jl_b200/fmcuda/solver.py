@@ -31,10 +31,12 @@ from .sources import PlaneWaveSource, as_list, source_wavelength
 @dataclass(frozen=True)
 class KrylovJL_GMRES:
     """GMRES as LinearSolve's KrylovJL_GMRES runs it (default: no restart).  ``gmres_restart`` > 0
-    gives GMRES(m).  ``ortho`` picks the Gram-Schmidt variant ("mgs" as Krylov.jl, "cgs", "cgs2");
+    gives GMRES(m).  ``ortho`` picks the Gram-Schmidt variant ("mgs" as Krylov.jl, "cgs", "cgs2", or "block":
+    s-step GMRES with ``block_size`` vectors per block, full GMRES only);
     None chooses MGS for FP64 (Krylov.jl's choice) and classical Gram-Schmidt for the FP32 forms."""
     gmres_restart: int = 0
     ortho: Optional[str] = None
+    block_size: int = 4
 
 
 @dataclass(frozen=True)
@@ -47,7 +49,7 @@ class BornSeries:
     """The plain convergent Born series (Richardson iteration on the preconditioned system)."""
 
 
-_ORTHO = {"mgs": L.FM_ORTHO_MGS, "cgs": L.FM_ORTHO_CGS, "cgs2": L.FM_ORTHO_CGS2}
+_ORTHO = {"mgs": L.FM_ORTHO_MGS, "cgs": L.FM_ORTHO_CGS, "cgs2": L.FM_ORTHO_CGS2, "block": L.FM_ORTHO_BLOCK}
 
 
 def _device_available() -> int:
@@ -146,6 +148,7 @@ class ConvergentBornSolver:
             o.method = L.FM_METHOD_GMRES
             ortho = ls.ortho or ("mgs" if self.precision == "float64" else "cgs")
             o.ortho = _ORTHO[ortho]
+            o.block = int(ls.block_size) if ortho == "block" else 0
             o.restart = int(ls.gmres_restart)
         elif isinstance(ls, KrylovJL_BICGSTAB):
             o.method = L.FM_METHOD_BICGSTAB

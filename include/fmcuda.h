@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FMCUDA_ABI_VERSION 1
+#define FMCUDA_ABI_VERSION 2
 
 typedef enum {
   FM_OK = 0,
@@ -43,7 +43,13 @@ typedef enum {
  * arithmetic carried out in FP64 registers. */
 enum { FM_PREC_F64 = 0, FM_PREC_F32 = 1, FM_PREC_F32_MATH64 = 2 };
 enum { FM_METHOD_GMRES = 0, FM_METHOD_BICGSTAB = 1, FM_METHOD_RICHARDSON = 2 };
-enum { FM_ORTHO_MGS = 0, FM_ORTHO_CGS = 1, FM_ORTHO_CGS2 = 2 };
+/* FM_ORTHO_BLOCK: s-step GMRES.  The first `block` iterations are classical Gram-Schmidt; after them each
+ * step builds `block` Krylov vectors with Newton shifts (Ritz values of the first steps) and orthogonalises
+ * them together against the basis, so the basis is read twice per `block` iterations instead of twice per
+ * iteration.  The Hessenberg matrix is recovered exactly from the block relations, so in exact arithmetic
+ * the iterate, residual estimates and stopping iteration are those of full GMRES.  Full GMRES only
+ * (restart = 0). */
+enum { FM_ORTHO_MGS = 0, FM_ORTHO_CGS = 1, FM_ORTHO_CGS2 = 2, FM_ORTHO_BLOCK = 3 };
 
 typedef struct fm_plan fm_plan;
 
@@ -69,6 +75,7 @@ typedef struct {
   double reltol;        /* solver.tolerance (convergent_born.jl:744) */
   double abstol;        /* solver.tolerance * 1e-2 (convergent_born.jl:745) */
   double timeout_s;     /* host-side deadline for the whole call, 0 = none */
+  int block;            /* FM_ORTHO_BLOCK: vectors per block, 2..5 (0: 4); ignored otherwise */
 } fm_solve_opts;
 
 typedef struct {

@@ -32,7 +32,7 @@ def test_library_exports_every_header_symbol():
 
 def test_library_loads_without_gpu_calls():
     L = _lib.lib()
-    assert L.fm_abi_version() == 1
+    assert L.fm_abi_version() == 2
     assert isinstance(L.fm_device_count(), int)
     assert L.fm_last_error() is not None
 
