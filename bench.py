@@ -386,7 +386,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fmcuda", choices=["fmcuda", "reference"])
     ap.add_argument("--nrhs", type=int, default=64)
-    ap.add_argument("--ortho", default="cgs", choices=["mgs", "cgs", "cgs2", "block"])
+    ap.add_argument("--ortho", default="block", choices=["mgs", "cgs", "cgs2", "block"])
     ap.add_argument("--block", type=int, default=4, help="vectors per block for --ortho block")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
     ap.add_argument("--e2e-steps", type=int, default=1)
@@ -394,7 +394,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--operator-case", action="store_true", help="profiling case: operator applications only")
     ap.add_argument("--reps", type=int, default=3)
-    ap.add_argument("--serving-requests", type=int, default=16, help="requests in the serving sample (0: skip)")
+    ap.add_argument("--serving-requests", type=int, default=8, help="requests in the serving sample (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
     ap.add_argument("--serving-basis", type=int, default=100)

@@ -509,6 +509,19 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate(long long M, int B, 
 // consecutive elements (32 bytes of complex FP32); the summed element index is
 // permuted in the same way for both operands, which leaves the products as they are.
 // ---------------------------------------------------------------------------
+// four consecutive complex values starting at a 32-byte aligned address (two or four 128-bit loads)
+__device__ __forceinline__ void load4(const float2* p, float2 (&v)[4]) {
+  const float4 a = reinterpret_cast<const float4*>(p)[0], c = reinterpret_cast<const float4*>(p)[1];
+  v[0] = make_float2(a.x, a.y);
+  v[1] = make_float2(a.z, a.w);
+  v[2] = make_float2(c.x, c.y);
+  v[3] = make_float2(c.z, c.w);
+}
+__device__ __forceinline__ void load4(const double2* p, double2 (&v)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = p[q];
+}
+
 __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c0), "+d"(c1)
@@ -564,10 +577,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
           xv[q].x = 0;
           xv[q].y = 0;
         }
-        if (k < K && ein) {
-#pragma unroll
-          for (int q = 0; q < 4; ++q) xv[q] = ub[(size_t)k * us + eb + q];
-        }
+        if (k < K && ein) load4(ub + (size_t)k * us + eb, xv);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const double2 x = to_d(xv[q]);
@@ -647,10 +657,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
         xv[q].x = 0;
         xv[q].y = 0;
       }
-      if (k < K && ein) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) xv[q] = ub[(size_t)k * us + ea + q];
-      }
+      if (k < K && ein) load4(ub + (size_t)k * us + ea, xv);
       const double bfr = Bs[k0 + tig][gid];  // rows past K are zero
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
