@@ -998,9 +998,10 @@ static cudaError_t block_kernels(fm_plan* P, bool dot, int S, int nb, int K, con
   }
 }
 
-// Block vectors are generated and kept in FP64 (YR = double) on FP64 and FP32-storage/FP64-arithmetic plans:
-// rounding the raw Krylov vectors to FP32 before they are orthogonalised is what costs accuracy in an s-step
-// basis.  The orthogonalised block is stored in the basis type.
+// Block vectors are generated and kept in FP64 (YR = double) on FP64 and FP32-storage/FP64-arithmetic plans
+// unless the caller asks for the plan's storage type (FM_BLOCK_STORAGE): rounding the raw Krylov vectors to FP32
+// before they are orthogonalised is what costs accuracy in an s-step basis.  The orthogonalised block is stored
+// in the basis type.
 template <typename R, typename YR>
 static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<fm_solve_info>& info,
                              double deadline) {
@@ -1553,8 +1554,8 @@ static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
   FM_CK(cudaMemcpyAsync(P->xbuf.p, P->bbuf.p, fbytes, cudaMemcpyDeviceToDevice, P->st));
   fm_status st;
   if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK)
-    st = P->prec == FM_PREC_F32 ? gmres_block<R, R>(P, nb, o, info, deadline)
-                                : gmres_block<R, double>(P, nb, o, info, deadline);
+    st = (P->c64 && o.block_store == FM_BLOCK_FP64) ? gmres_block<R, double>(P, nb, o, info, deadline)
+                                                    : gmres_block<R, R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_GMRES) st = gmres<R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_BICGSTAB) st = bicgstab<R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_RICHARDSON) st = richardson<R>(P, nb, o, info, deadline);
@@ -1603,6 +1604,8 @@ static fm_status validate_opts(const fm_solve_opts* o) {
   if (o->ortho < 0 || o->ortho > 3) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
   if (o->ortho == FM_ORTHO_BLOCK && o->method == FM_METHOD_GMRES) {
     if (o->block != 0 && (o->block < 2 || o->block > 5)) return fail(FM_ERR_INVALID, "block size must be 2..5");
+    if (o->block_store != FM_BLOCK_FP64 && o->block_store != FM_BLOCK_STORAGE)
+      return fail(FM_ERR_INVALID, "unknown block vector storage");
     if (o->restart > 0) return fail(FM_ERR_UNSUPPORTED, "block GMRES runs full GMRES only (restart = 0)");
     if (o->maxiters + block_size_of(*o) + 1 > KV_KMAX)
       return fail(FM_ERR_UNSUPPORTED, "GMRES basis larger than 128 vectors");
@@ -1625,7 +1628,8 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   size_t extra = 0;  // block GMRES: FP64 block vectors, FP64 pass temporaries, FP64 potential
   if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK) {
     vecs = o.maxiters + block_size_of(o) + 1;
-    extra = (size_t)P->M * sizeof(double2) * (block_size_of(o) + 1 + 2);
+    extra = (o.block_store == FM_BLOCK_FP64 && P->c64) ? (size_t)P->M * sizeof(double2) * (block_size_of(o) + 1 + 2)
+                                                        : fb * (size_t)(block_size_of(o) + 1);
   }
   else if (o.method == FM_METHOD_BICGSTAB) vecs = 6;
   else vecs = 1;

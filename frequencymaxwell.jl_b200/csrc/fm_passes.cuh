@@ -58,7 +58,7 @@ __device__ __forceinline__ void load_table(T* dst, const T* src, int n) {
 enum { PRO_COPY = 0, PRO_V = 1, PRO_V_SCALE = 2 };
 
 template <typename S, typename R, int L, int PRO>
-__global__ void __launch_bounds__(256) k_xf(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
+__global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xf(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
                                             const double* __restrict__ rhs_scale, const cplx<R>* __restrict__ twx,
                                             const cplx<R>* __restrict__ rampx, cplx<S>* __restrict__ out,
                                             const int* __restrict__ active, VecTab vt) {
@@ -333,7 +333,7 @@ struct EpiParams {
 };
 
 template <typename S, typename R, int L, int EPI>
-__global__ void __launch_bounds__(256) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
+__global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
                                             const cplx<S>* __restrict__ xv, const cplx<S>* __restrict__ bv,
                                             const double* __restrict__ rhs_scale, EpiParams ep,
                                             const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ rampx,

@@ -18,6 +18,7 @@ FM_OK, FM_ERR_INVALID, FM_ERR_OOM, FM_NOT_CONVERGED, FM_ERR_NONFINITE, FM_ERR_TI
 FM_PREC_F64, FM_PREC_F32, FM_PREC_F32_MATH64 = 0, 1, 2
 FM_METHOD_GMRES, FM_METHOD_BICGSTAB, FM_METHOD_RICHARDSON = 0, 1, 2
 FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2, FM_ORTHO_BLOCK = 0, 1, 2, 3
+FM_BLOCK_FP64, FM_BLOCK_STORAGE = 0, 1
 
 STATUS_NAMES = {
     FM_OK: "FM_OK", FM_ERR_INVALID: "FM_ERR_INVALID", FM_ERR_OOM: "FM_ERR_OOM",
@@ -43,7 +44,8 @@ class fm_plan_desc(C.Structure):
 
 class fm_solve_opts(C.Structure):
     _fields_ = [("method", C.c_int), ("ortho", C.c_int), ("restart", C.c_int), ("maxiters", C.c_int),
-                ("reltol", C.c_double), ("abstol", C.c_double), ("timeout_s", C.c_double), ("block", C.c_int)]
+                ("reltol", C.c_double), ("abstol", C.c_double), ("timeout_s", C.c_double), ("block", C.c_int),
+                ("block_store", C.c_int)]
 
 
 class fm_solve_info(C.Structure):

@@ -32,11 +32,13 @@ from .sources import PlaneWaveSource, as_list, source_wavelength
 class KrylovJL_GMRES:
     """GMRES as LinearSolve's KrylovJL_GMRES runs it (default: no restart).  ``gmres_restart`` > 0
     gives GMRES(m).  ``ortho`` picks the Gram-Schmidt variant ("mgs" as Krylov.jl, "cgs", "cgs2", or "block":
-    s-step GMRES with ``block_size`` vectors per block, full GMRES only);
+    s-step GMRES with ``block_size`` vectors per block, full GMRES only; ``block_vectors`` "fp64" keeps the raw
+    block vectors in complex FP64 on plans that compute in FP64, "storage" in the plan's storage type);
     None chooses MGS for FP64 (Krylov.jl's choice) and classical Gram-Schmidt for the FP32 forms."""
     gmres_restart: int = 0
     ortho: Optional[str] = None
     block_size: int = 4
+    block_vectors: str = "fp64"
 
 
 @dataclass(frozen=True)
@@ -149,6 +151,7 @@ class ConvergentBornSolver:
             ortho = ls.ortho or ("mgs" if self.precision == "float64" else "cgs")
             o.ortho = _ORTHO[ortho]
             o.block = int(ls.block_size) if ortho == "block" else 0
+            o.block_store = {"fp64": L.FM_BLOCK_FP64, "storage": L.FM_BLOCK_STORAGE}[ls.block_vectors]
             o.restart = int(ls.gmres_restart)
         elif isinstance(ls, KrylovJL_BICGSTAB):
             o.method = L.FM_METHOD_BICGSTAB

@@ -40,6 +40,7 @@ struct FMSolveOpts
     abstol::Cdouble
     timeout_s::Cdouble
     block::Cint
+    block_store::Cint
 end
 
 struct FMSolveInfo
@@ -125,7 +126,7 @@ function solve_fmcuda(solver::ConvergentBornSolver{T}, sources, medium) where {T
         first = Cint[0, length(waves)]
         method = solver.linear_solver isa LinearSolve.KrylovJL && occursin("bicgstab", lowercase(string(solver.linear_solver.KrylovAlg))) ? Cint(1) : Cint(0)
         opts = Ref(FMSolveOpts(method, T === Float64 ? Cint(0) : Cint(1), Cint(0), Cint(max(2bornmax, 100)),
-                               solver.tolerance, solver.tolerance * 1e-2, 0.0, Cint(0)))
+                               solver.tolerance, solver.tolerance * 1e-2, 0.0, Cint(0), Cint(0)))
         E = Array{ComplexF64}(undef, solver.grid_size..., 3)
         H = similar(E)
         info = Ref{FMSolveInfo}()

@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 SOLVE_TOL = {"float64": 1e-10, "float32": 1e-5, "float32-math64": 1e-5}
 
 
-def _solve(grid, radius, precision, block, tol=1e-6, sources=None):
-    ls = F.KrylovJL_GMRES(ortho="block", block_size=block)
+def _solve(grid, radius, precision, block, tol=1e-6, sources=None, store="fp64"):
+    ls = F.KrylovJL_GMRES(ortho="block", block_size=block, block_vectors=store)
     ocfg, solver = configs(grid, absorbing_z(grid[2]), tol=tol, precision=precision, linear_solver=ls)
     eps = bead(grid, radius)
     osrc, fsrc = sources if sources is not None else xpol()
@@ -71,11 +71,13 @@ def test_block_gmres_batch_equals_single():
             assert rel(o.H, one.H) < 1e-12
 
 
-def test_block_gmres_oblique_fp32_math64():
+@pytest.mark.parametrize("store", ["fp64", "storage"])
+def test_block_gmres_oblique_fp32_math64(store):
+    """Both kinds of raw block vectors on the FP32-storage / FP64-arithmetic plan."""
     grid = (32, 32, 16)
     src = F.illumination_cone(grid, (50e-9,) * 3, WL, EPS_BG, 4, 1.2, 11)[3]
     pair = (O.PlaneWave(WL, src.polarization, src.k_vector), src)
-    ref, out, _ = _solve(grid, 5.0, "float32-math64", 4, sources=pair)
+    ref, out, _ = _solve(grid, 5.0, "float32-math64", 4, sources=pair, store=store)
     assert rel(out.E, ref.E) < 1e-5
     assert rel(out.H, ref.H) < 1e-5
 
