@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   double P[GPW][2], Q[GPW][2];
 #pragma unroll
   for (int g = 0; g < GPW; ++g) P[g][0] = P[g][1] = Q[g][0] = Q[g][1] = 0.0;
-  const long long per = ((M + nblk - 1) / nblk + 15) / 16 * 16;
+  const long long per = ((M + nblk - 1) / nblk + 31) / 32 * 32;
   const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
   const size_t us = (size_t)B * M;
   const T* ub = U + (size_t)b * M;
@@ -555,35 +555,45 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   const int yt = gid & 3;                   // block vector of this lane's B column
   const bool yim = gid >= 4, yon = yt < S;  // imaginary part / column in use
   if (ew < EW) {
-    for (long long e0 = lo + (long long)ew * 16; e0 < hi; e0 += (long long)EW * 16) {
-      const long long eb = e0 + 4 * tig;  // this lane's run of 4 elements (wholly inside or outside)
-      const bool ein = eb < hi;
-      double bf[4];
+    // a warp step covers 32 elements: two runs of 4 per lane (h = 0, 1), i.e. twice the loads in flight
+    for (long long e0 = lo + (long long)ew * 32; e0 < hi; e0 += (long long)EW * 32) {
+      double bf[2][4];
+      bool ein[2];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        bf[q] = 0.0;
-        if (yon && ein) {
-          const double2 y = to_d(yb[yt * us + eb + q]);
-          bf[q] = yim ? y.y : y.x;
+      for (int h = 0; h < 2; ++h) {
+        const long long eb = e0 + 16 * h + 4 * tig;  // wholly inside or outside the range
+        ein[h] = eb < hi;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          bf[h][q] = 0.0;
+          if (yon && ein[h]) {
+            const double2 y = to_d(yb[yt * us + eb + q]);
+            bf[h][q] = yim ? y.y : y.x;
+          }
         }
       }
 #pragma unroll
       for (int g = 0; g < GPW; ++g) {
         if ((kw * GPW + g) >= KG) break;  // warp-uniform
         const int k = (kw * GPW + g) * 8 + gid;
-        T xv[4];
+        T xv[2][4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          xv[q].x = 0;
-          xv[q].y = 0;
-        }
-        if (k < K && ein) load4(ub + (size_t)k * us + eb, xv);
+        for (int h = 0; h < 2; ++h) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const double2 x = to_d(xv[q]);
-          mma_f64(P[g][0], P[g][1], x.x, bf[q]);
-          mma_f64(Q[g][0], Q[g][1], x.y, bf[q]);
+          for (int q = 0; q < 4; ++q) {
+            xv[h][q].x = 0;
+            xv[h][q].y = 0;
+          }
+          if (k < K && ein[h]) load4(ub + (size_t)k * us + e0 + 16 * h + 4 * tig, xv[h]);
         }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const double2 x = to_d(xv[h][q]);
+            mma_f64(P[g][0], P[g][1], x.x, bf[h][q]);
+            mma_f64(Q[g][0], Q[g][1], x.y, bf[h][q]);
+          }
       }
     }
   }
