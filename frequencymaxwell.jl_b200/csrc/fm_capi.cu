@@ -904,45 +904,19 @@ template <typename R, typename YR, int S>
 static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, const void* Y, const int* act, int nact) {
   using T = cplx<R>;
   using TY = cplx<YR>;
-  int nblk = 1;
-  size_t smem = 0;
-  if constexpr (S <= 4) {
-    int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
-        bps < 1)
-      bps = 1;
-    const long long maxb = (P->M + 127) / 128;
-    nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
-  } else {
-    smem = blockdot_smem<R, TY>(K, S);
-    static bool attr = false;  // one instantiation per (R, TY, S): raise its dynamic shared memory limit once
-    if (!attr) {
-      cudaError_t ea = cudaFuncSetAttribute(k_blockdot<R, TY, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)blockdot_smem<R, TY>(KV_KMAX, S));
-      if (ea != cudaSuccess) return ea;
-      attr = true;
-    }
-    int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot<R, TY, S>, KV_THREADS, smem) != cudaSuccess ||
-        bps < 1)
-      bps = 1;
-    const long long maxb = (P->M + KB_TE - 1) / KB_TE;
-    nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
-  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
+      bps < 1)
+    bps = 1;
+  const long long maxb = (P->M + 127) / 128;
+  const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   cudaError_t e = P->red_part.ensure((size_t)nb * nblk * K * S * sizeof(double2));
   if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
   if (e != cudaSuccess) return e;
-  const double bytes = ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
-  if constexpr (S <= 4)
-    FM_TRACK(P, KC_DOT, bytes,
-             (k_blockdot_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-                 P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
-                 (unsigned*)P->red_cnt.p, act)));
-  else
-    FM_TRACK(P, KC_DOT, bytes,
-             (k_blockdot<R, TY, S><<<dim3(nblk, nb), KV_THREADS, smem, P->st>>>(
-                 P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
-                 (unsigned*)P->red_cnt.p, act)));
+  FM_TRACK(P, KC_DOT, ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M,
+           (k_blockdot_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
+               (unsigned*)P->red_cnt.p, act)));
   return cudaGetLastError();
 }
 
@@ -952,29 +926,15 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
   using T = cplx<R>;
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
-  const double bytes = ((double)(K + S) * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
-  if constexpr (S <= 4) {
-    int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S>, KV_THREADS, 0) !=
-            cudaSuccess ||
-        bps < 1)
-      bps = 1;
-    const long long maxb = (P->M + 32 * KV_WARPS - 1) / (32 * KV_WARPS);
-    const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
-    FM_TRACK(P, KC_UPD, bytes,
-             (k_blockupdate_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-                 P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
-  } else {
-    int bps = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
-        bps < 1)
-      bps = 1;
-    const long long maxb = (P->M + KV_THREADS / KB_KS - 1) / (KV_THREADS / KB_KS);
-    const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
-    FM_TRACK(P, KC_UPD, bytes,
-             (k_blockupdate<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-                 P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
-  }
+  int bps = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
+      bps < 1)
+    bps = 1;
+  const long long maxb = (P->M + 32 * KV_WARPS - 1) / (32 * KV_WARPS);
+  const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+  FM_TRACK(P, KC_UPD, ((double)(K + S) * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M,
+           (k_blockupdate_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int nblk_g = kv_blocks(P, k_blockgram<R, S>, nb);
@@ -994,6 +954,9 @@ static cudaError_t block_kernels(fm_plan* P, bool dot, int S, int nb, int K, con
     case 3: return dot ? launch_blockdot<R, YR, 3>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 3>(P, nb, K, U, Y, Z, act, nact);
     case 4: return dot ? launch_blockdot<R, YR, 4>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 4>(P, nb, K, U, Y, Z, act, nact);
     case 5: return dot ? launch_blockdot<R, YR, 5>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 5>(P, nb, K, U, Y, Z, act, nact);
+    case 6: return dot ? launch_blockdot<R, YR, 6>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 6>(P, nb, K, U, Y, Z, act, nact);
+    case 7: return dot ? launch_blockdot<R, YR, 7>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 7>(P, nb, K, U, Y, Z, act, nact);
+    case 8: return dot ? launch_blockdot<R, YR, 8>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 8>(P, nb, K, U, Y, Z, act, nact);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -1603,7 +1566,7 @@ static fm_status validate_opts(const fm_solve_opts* o) {
   if (o->method < 0 || o->method > 2) return fail(FM_ERR_INVALID, "unknown method");
   if (o->ortho < 0 || o->ortho > 3) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
   if (o->ortho == FM_ORTHO_BLOCK && o->method == FM_METHOD_GMRES) {
-    if (o->block != 0 && (o->block < 2 || o->block > 5)) return fail(FM_ERR_INVALID, "block size must be 2..5");
+    if (o->block != 0 && (o->block < 2 || o->block > 8)) return fail(FM_ERR_INVALID, "block size must be 2..8");
     if (o->block_store != FM_BLOCK_FP64 && o->block_store != FM_BLOCK_STORAGE)
       return fail(FM_ERR_INVALID, "unknown block vector storage");
     if (o->restart > 0) return fail(FM_ERR_UNSUPPORTED, "block GMRES runs full GMRES only (restart = 0)");

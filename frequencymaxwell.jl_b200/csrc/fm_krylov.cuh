@@ -312,196 +312,14 @@ __global__ void __launch_bounds__(KV_THREADS) k_combine(long long M, int B, int 
     ob[e] = from_d<TY>(acc);
   }
 }
-// Block dot tiles hold the basis values widened to complex FP64 (16 bytes each): KB_TE values per row,
-// value c of row k stored at position c ^ (k & 7), so eight lanes reading the same column of eight
-// consecutive rows hit eight different 16-byte bank groups.  Each basis value is widened once, when it
-// is staged; the inner loop only reads FP64 values.
-constexpr int KB_TE = 32;
-constexpr int KB_PF = KV_KMAX * KB_TE / KV_THREADS;  // staged values per thread and tile, at most
-
-template <typename R, typename TY>
-__host__ __device__ constexpr size_t blockdot_smem(int K, int S) {
-  return (size_t)K * KB_TE * sizeof(double2) + (size_t)S * KB_TE * sizeof(double2) >
-                 (size_t)KV_THREADS * S * sizeof(double2)
-             ? (size_t)K * KB_TE * sizeof(double2) + (size_t)S * KB_TE * sizeof(double2)
-             : (size_t)KV_THREADS * S * sizeof(double2);
-}
-
-// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 accumulation, deterministic)
-// The block streams its element range in tiles of KB_TE elements of the K basis vectors and the S block
-// vectors.  The next tile is loaded into registers while this one is used from shared memory; each
-// thread owns one basis vector k (and a share of the tile's elements) and keeps its S dot products in
-// registers across all tiles: no per-tile cross-lane reduction.
-template <typename R, typename TY, int S>
-__global__ void __launch_bounds__(KV_THREADS) k_blockdot(long long M, int B, int K, const cplx<R>* __restrict__ U,
-                                                         const TY* __restrict__ Y, double2* __restrict__ part,
-                                                         double2* __restrict__ out, unsigned* __restrict__ counter,
-                                                         const int* __restrict__ active) {
-  using T = cplx<R>;
-  extern __shared__ __align__(16) unsigned char kb_smem[];
-  double2* Xs = reinterpret_cast<double2*>(kb_smem);   // [K][KB_TE], swizzled
-  double2* Ys = Xs + (size_t)K * KB_TE;                 // [S][KB_TE]
-  const int b = blockIdx.y, nblk = gridDim.x;
-  if (active && !active[b]) return;
-  const int Kp = (K + 31) & ~31;
-  const int G = KV_THREADS / Kp;
-  const int k = threadIdx.x % Kp, pr = threadIdx.x / Kp;
-  double2 acc[S];
-#pragma unroll
-  for (int t = 0; t < S; ++t) acc[t] = make_double2(0.0, 0.0);
-  const long long per = ((M + nblk - 1) / nblk + KB_TE - 1) / KB_TE * KB_TE;
-  const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
-  const size_t us = (size_t)B * M;
-  // staging: thread copies column sc = tid % KB_TE of rows sr, sr + 8, ...
-  const int sc = threadIdx.x % KB_TE, sr = threadIdx.x / KB_TE;
-  constexpr int RS = KV_THREADS / KB_TE;  // rows per staging pass
-  const T* xsrc = U + (size_t)b * M + (size_t)sr * us + sc;
-  const TY* ysrc = Y + (size_t)b * M;
-  T xr[KB_PF];
-  TY yr = TY{};
-  auto load = [&](long long e0) {
-    const bool v = e0 + sc < hi;
-#pragma unroll
-    for (int j = 0; j < KB_PF; ++j) {
-      xr[j].x = 0;
-      xr[j].y = 0;
-      if (v && sr + j * RS < K) xr[j] = xsrc[e0 + (size_t)j * RS * us];
-    }
-    if (threadIdx.x < S * KB_TE) {
-      const int t = threadIdx.x / KB_TE;
-      yr.x = 0;
-      yr.y = 0;
-      if (v) yr = ysrc[t * us + e0 + sc];
-    }
-  };
-  auto store = [&]() {
-#pragma unroll
-    for (int j = 0; j < KB_PF; ++j) {
-      const int kk = sr + j * RS;
-      if (kk < K) Xs[kk * KB_TE + (sc ^ (kk & 7))] = to_d(xr[j]);
-    }
-    if (threadIdx.x < S * KB_TE) Ys[threadIdx.x] = to_d(yr);
-  };
-  if (lo < hi) load(lo);
-  for (long long e0 = lo; e0 < hi; e0 += KB_TE) {
-    __syncthreads();  // the previous tile has been used
-    store();
-    __syncthreads();
-    if (e0 + KB_TE < hi) load(e0 + KB_TE);  // in flight while this tile is used
-    if (k < K) {
-      const double2* row = Xs + (size_t)k * KB_TE;
-      for (int c = pr; c < KB_TE; c += G) {
-        const double2 u = row[c ^ (k & 7)];
-#pragma unroll
-        for (int t = 0; t < S; ++t) {
-          const double2 y = Ys[t * KB_TE + c];
-          acc[t].x = fma(u.x, y.x, fma(u.y, y.y, acc[t].x));
-          acc[t].y = fma(u.x, y.y, fma(-u.y, y.x, acc[t].y));
-        }
-      }
-    }
-  }
-  __syncthreads();
-  double2* red = reinterpret_cast<double2*>(kb_smem);  // [KV_THREADS][S]
-#pragma unroll
-  for (int t = 0; t < S; ++t) red[threadIdx.x * S + t] = acc[t];
-  __syncthreads();
-  const int KS = K * S;
-  for (int o = threadIdx.x; o < KS; o += blockDim.x) {
-    const int kk = o / S, t = o - kk * S;
-    double2 sum = make_double2(0.0, 0.0);
-    for (int q = 0; q < G; ++q) {
-      const double2 v = red[(q * Kp + kk) * S + t];
-      sum.x += v.x;
-      sum.y += v.y;
-    }
-    part[((size_t)b * nblk + blockIdx.x) * KS + o] = sum;
-  }
-  finish_reduce(part, out, counter, KS, nblk, b);
-}
-
-// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  for t < S (FP64 accumulation; Z_t stored in the basis
-// type at Z[(t*B + b)*M]).  KB_KS threads share each element, thread q summing the basis vectors
-// k = q, q + KB_KS, ...: short dependency chains and KB_KS times more elements in flight per register.
-// The partial sums meet in shared memory.
-constexpr int KB_KS = 4;
-template <typename R, typename TY, int S>
-__global__ void __launch_bounds__(KV_THREADS) k_blockupdate(long long M, int B, int K, const cplx<R>* U, const TY* Y,
-                                                            cplx<R>* Z, const double2* __restrict__ coef,
-                                                            const int* __restrict__ active) {
-  using T = cplx<R>;
-  constexpr int NE = KV_THREADS / KB_KS;  // elements per block round
-  constexpr int KU = 4;                   // loads in flight per thread
-  __shared__ double2 cs[KV_KMAX * S];
-  __shared__ double2 red[KB_KS - 1][S][NE];
-  const int b = blockIdx.y;
-  if (active && !active[b]) return;
-  for (int i = threadIdx.x; i < K * S; i += blockDim.x) cs[i] = coef[(size_t)b * KV_KMAX * S + i];
-  __syncthreads();
-  const int el = threadIdx.x % NE, q = threadIdx.x / NE;
-  const TY* yb = Y + (size_t)b * M;
-  T* zb = Z + (size_t)b * M;
-  const size_t us = (size_t)B * M;
-  const T* ub = U + (size_t)b * M + (size_t)q * us;
-  const long long rounds = (M + NE - 1) / NE;
-  for (long long r = blockIdx.x; r < rounds; r += gridDim.x) {
-    const long long e = r * NE + el;
-    const bool in = e < M;
-    double2 acc[S];
-#pragma unroll
-    for (int t = 0; t < S; ++t) acc[t] = make_double2(0.0, 0.0);
-    const T* xp = ub + e;
-    for (int k = q; k < K; k += KB_KS * KU) {
-      T xr[KU];
-#pragma unroll
-      for (int u = 0; u < KU; ++u) {
-        xr[u].x = 0;
-        xr[u].y = 0;
-        if (in && k + u * KB_KS < K) xr[u] = xp[(size_t)(k - q + u * KB_KS) * us];
-      }
-#pragma unroll
-      for (int u = 0; u < KU; ++u) {
-        const int kk = k + u * KB_KS;
-        if (kk >= K) break;
-        const double2 x = to_d(xr[u]);
-#pragma unroll
-        for (int t = 0; t < S; ++t) {
-          const double2 c = cs[kk * S + t];
-          acc[t].x = fma(c.x, x.x, fma(-c.y, x.y, acc[t].x));
-          acc[t].y = fma(c.x, x.y, fma(c.y, x.x, acc[t].y));
-        }
-      }
-    }
-    if (q > 0) {
-#pragma unroll
-      for (int t = 0; t < S; ++t) red[q - 1][t][el] = acc[t];
-    }
-    __syncthreads();
-    if (q == 0 && in) {
-#pragma unroll
-      for (int t = 0; t < S; ++t) {
-        double2 v = to_d(yb[t * us + e]);
-        v.x -= acc[t].x;
-        v.y -= acc[t].y;
-#pragma unroll
-        for (int qq = 0; qq < KB_KS - 1; ++qq) {
-          v.x -= red[qq][t][el].x;
-          v.y -= red[qq][t][el].y;
-        }
-        zb[t * us + e] = from_d<T>(v);
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // FP64 tensor-core (mma.sync m8n8k4 .f64) forms of the block dot and block
-// update, for S <= 4 block vectors.  The real and imaginary parts of the S
-// block vectors (or coefficients) fill the 8 columns of the B operand (columns
-// t: real part of vector t, 4 + t: imaginary part; columns of t >= S are zero),
-// and the real and imaginary parts of the basis values are the A operands of two
-// MMAs, P and Q, so that for column t
+// update.  For S <= 4 the real and imaginary parts of the S block vectors (or
+// coefficients) fill the 8 columns of the B operand (columns t: real part of
+// vector t, 4 + t: imaginary part; columns of t >= S are zero); for S <= 8 two
+// B tiles hold the real and the imaginary parts.  The real and imaginary parts of
+// the basis values are the A operands of two MMAs per tile, P and Q, so that for
+// column t (one tile)
 //   conj(x) y:  Re = P[t] + Q[4+t],   Im = P[4+t] - Q[t]
 //   x c:        Re = P[t] - Q[4+t],   Im = P[4+t] + Q[t].
 // Fragment layout of m8n8k4 (row.col): A[gid][tig], B[tig][gid] and
@@ -528,15 +346,18 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
                : "d"(a), "d"(b));
 }
 
-// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 4)
+// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 8)
+// S <= 4: one B tile; S > 4: two tiles (tile 0: Re Y_t, tile 1: Im Y_t, column t), so that
+//   Re = P0[t] + Q1[t],  Im = P1[t] - Q0[t]  within each lane.
 template <typename R, typename TY, int S>
 __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B, int K, const cplx<R>* __restrict__ U,
                                                              const TY* __restrict__ Y, double2* __restrict__ part,
                                                              double2* __restrict__ out, unsigned* __restrict__ counter,
                                                              const int* __restrict__ active) {
-  static_assert(S <= 4, "block dot on tensor cores takes at most 4 block vectors");
+  static_assert(S >= 1 && S <= 8, "block dot on tensor cores takes 1..8 block vectors");
   using T = cplx<R>;
-  constexpr int GPW = 4;  // groups of 8 basis vectors per warp
+  constexpr int NT = S <= 4 ? 1 : 2;   // 8-column B tiles
+  constexpr int GPW = S <= 4 ? 4 : 2;  // groups of 8 basis vectors per warp
   __shared__ double2 red[KV_WARPS][GPW * 8][S];
   const int b = blockIdx.y, nblk = gridDim.x;
   if (active && !active[b]) return;
@@ -544,20 +365,22 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   const int gid = lane >> 2, tig = lane & 3;
   const int KG = (K + 7) >> 3, KW = (KG + GPW - 1) / GPW, EW = KV_WARPS / KW;
   const int kw = w % KW, ew = w / KW;
-  double P[GPW][2], Q[GPW][2];
+  double P[GPW][NT][2], Q[GPW][NT][2];
 #pragma unroll
-  for (int g = 0; g < GPW; ++g) P[g][0] = P[g][1] = Q[g][0] = Q[g][1] = 0.0;
+  for (int g = 0; g < GPW; ++g)
+#pragma unroll
+    for (int n = 0; n < NT; ++n) P[g][n][0] = P[g][n][1] = Q[g][n][0] = Q[g][n][1] = 0.0;
   const long long per = ((M + nblk - 1) / nblk + 31) / 32 * 32;
   const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
   const size_t us = (size_t)B * M;
   const T* ub = U + (size_t)b * M;
   const TY* yb = Y + (size_t)b * M;
-  const int yt = gid & 3;                   // block vector of this lane's B column
-  const bool yim = gid >= 4, yon = yt < S;  // imaginary part / column in use
+  const int yt = NT == 1 ? (gid & 3) : gid;  // block vector of this lane's B column
+  const bool yon = yt < S;
   if (ew < EW) {
     // a warp step covers 32 elements: two runs of 4 per lane (h = 0, 1), i.e. twice the loads in flight
     for (long long e0 = lo + (long long)ew * 32; e0 < hi; e0 += (long long)EW * 32) {
-      double bf[2][4];
+      double bf[NT][2][4];
       bool ein[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
@@ -565,10 +388,13 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
         ein[h] = eb < hi;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          bf[h][q] = 0.0;
-          if (yon && ein[h]) {
-            const double2 y = to_d(yb[yt * us + eb + q]);
-            bf[h][q] = yim ? y.y : y.x;
+          double2 y = make_double2(0.0, 0.0);
+          if (yon && ein[h]) y = to_d(yb[yt * us + eb + q]);
+          if constexpr (NT == 1) {
+            bf[0][h][q] = gid >= 4 ? y.y : y.x;
+          } else {
+            bf[0][h][q] = y.x;
+            bf[NT - 1][h][q] = y.y;
           }
         }
       }
@@ -591,21 +417,32 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const double2 x = to_d(xv[h][q]);
-            mma_f64(P[g][0], P[g][1], x.x, bf[h][q]);
-            mma_f64(Q[g][0], Q[g][1], x.y, bf[h][q]);
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+              mma_f64(P[g][n][0], P[g][n][1], x.x, bf[n][h][q]);
+              mma_f64(Q[g][n][0], Q[g][n][1], x.y, bf[n][h][q]);
+            }
           }
       }
     }
   }
-  // columns 2 tig, 2 tig + 1 of P and Q; the partner lane tig ^ 2 holds columns 4 + (2 tig, 2 tig + 1)
 #pragma unroll
   for (int g = 0; g < GPW; ++g) {
-    const double pp0 = __shfl_xor_sync(0xffffffffu, P[g][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[g][1], 2);
-    const double qp0 = __shfl_xor_sync(0xffffffffu, Q[g][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[g][1], 2);
-    if (tig < 2) {
-      const int t0 = 2 * tig;
-      if (t0 < S) red[w][g * 8 + gid][t0] = make_double2(P[g][0] + qp0, pp0 - Q[g][0]);
-      if (t0 + 1 < S) red[w][g * 8 + gid][t0 + 1] = make_double2(P[g][1] + qp1, pp1 - Q[g][1]);
+    if constexpr (NT == 1) {
+      // columns 2 tig, 2 tig + 1 of P and Q; the partner lane tig ^ 2 holds columns 4 + (2 tig, 2 tig + 1)
+      const double pp0 = __shfl_xor_sync(0xffffffffu, P[g][0][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[g][0][1], 2);
+      const double qp0 = __shfl_xor_sync(0xffffffffu, Q[g][0][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[g][0][1], 2);
+      if (tig < 2) {
+        const int t0 = 2 * tig;
+        if (t0 < S) red[w][g * 8 + gid][t0] = make_double2(P[g][0][0] + qp0, pp0 - Q[g][0][0]);
+        if (t0 + 1 < S) red[w][g * 8 + gid][t0 + 1] = make_double2(P[g][0][1] + qp1, pp1 - Q[g][0][1]);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int t = 2 * tig + i;
+        if (t < S) red[w][g * 8 + gid][t] = make_double2(P[g][0][i] + Q[g][NT - 1][i], P[g][NT - 1][i] - Q[g][0][i]);
+      }
     }
   }
   __syncthreads();
@@ -624,24 +461,29 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   finish_reduce(part, out, counter, KS, nblk, b);
 }
 
-// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 4).  A warp owns 32
-// elements (lane gid: elements 4 gid .. 4 gid + 3 of the tile) and runs over the basis 4 vectors at a time.
+// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 8).  A warp owns 32 elements
+// (lane gid: elements 4 gid .. 4 gid + 3 of the tile) and runs over the basis 4 vectors at a time.  B tiles
+// as in k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or  Re = P0[t] - Q1[t],
+// Im = P1[t] + Q0[t]  (two tiles).
 template <typename R, typename TY, int S>
 __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, cplx<R>* Z,
                                                                 const double2* __restrict__ coef,
                                                                 const int* __restrict__ active) {
-  static_assert(S <= 4, "block update on tensor cores takes at most 4 block vectors");
+  static_assert(S >= 1 && S <= 8, "block update on tensor cores takes 1..8 block vectors");
   using T = cplx<R>;
-  __shared__ double Bs[KV_KMAX][8];  // B[k][col]: col t = Re E[k][t], 4 + t = Im E[k][t]
+  constexpr int NT = S <= 4 ? 1 : 2;
+  __shared__ double Bs[KV_KMAX][8 * NT];
   const int b = blockIdx.y;
   if (active && !active[b]) return;
-  for (int i = threadIdx.x; i < KV_KMAX * 8; i += blockDim.x) {
-    const int k = i >> 3, col = i & 7, t = col & 3;
+  for (int i = threadIdx.x; i < KV_KMAX * 8 * NT; i += blockDim.x) {
+    const int k = i / (8 * NT), col = i - k * (8 * NT);
+    const int t = NT == 1 ? (col & 3) : (col & 7);
+    const bool im = NT == 1 ? (col >= 4) : (col >= 8);
     double v = 0.0;
     if (k < K && t < S) {
       const double2 c = coef[(size_t)b * KV_KMAX * S + k * S + t];
-      v = col >= 4 ? c.y : c.x;
+      v = im ? c.y : c.x;
     }
     Bs[k][col] = v;
   }
@@ -656,9 +498,11 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
   for (long long tl = (long long)blockIdx.x * KV_WARPS + w; tl < tiles; tl += (long long)gridDim.x * KV_WARPS) {
     const long long ea = tl * 32 + 4 * gid;  // A rows of this lane: elements ea .. ea + 3 (wholly in or out)
     const bool ein = ea < M;
-    double P[4][2], Q[4][2];
+    double P[4][NT][2], Q[4][NT][2];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) P[q][0] = P[q][1] = Q[q][0] = Q[q][1] = 0.0;
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int n = 0; n < NT; ++n) P[q][n][0] = P[q][n][1] = Q[q][n][0] = Q[q][n][1] = 0.0;
     for (int k0 = 0; k0 < K; k0 += 4) {
       const int k = k0 + tig;
       T xv[4];
@@ -668,30 +512,46 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
         xv[q].y = 0;
       }
       if (k < K && ein) load4(ub + (size_t)k * us + ea, xv);
-      const double bfr = Bs[k0 + tig][gid];  // rows past K are zero
+      double bfr[NT];
+#pragma unroll
+      for (int n = 0; n < NT; ++n) bfr[n] = Bs[k0 + tig][8 * n + gid];  // rows past K are zero
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const double2 x = to_d(xv[q]);
-        mma_f64(P[q][0], P[q][1], x.x, bfr);
-        mma_f64(Q[q][0], Q[q][1], x.y, bfr);
+#pragma unroll
+        for (int n = 0; n < NT; ++n) {
+          mma_f64(P[q][n][0], P[q][n][1], x.x, bfr[n]);
+          mma_f64(Q[q][n][0], Q[q][n][1], x.y, bfr[n]);
+        }
       }
     }
     // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const double pp0 = __shfl_xor_sync(0xffffffffu, P[q][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[q][1], 2);
-      const double qp0 = __shfl_xor_sync(0xffffffffu, Q[q][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[q][1], 2);
-      // C row gid is element tl*32 + 4*gid + q, i.e. this lane's own A row q
       const long long e = ea + q;
-      if (tig < 2 && ein) {
-        const int t0 = 2 * tig;
-        if (t0 < S) {
-          const double2 y = to_d(yb[t0 * us + e]);
-          zb[t0 * us + e] = from_d<T>(make_double2(y.x - (P[q][0] - qp0), y.y - (pp0 + Q[q][0])));
+      if constexpr (NT == 1) {
+        const double pp0 = __shfl_xor_sync(0xffffffffu, P[q][0][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[q][0][1], 2);
+        const double qp0 = __shfl_xor_sync(0xffffffffu, Q[q][0][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[q][0][1], 2);
+        if (tig < 2 && ein) {
+          const int t0 = 2 * tig;
+          if (t0 < S) {
+            const double2 y = to_d(yb[t0 * us + e]);
+            zb[t0 * us + e] = from_d<T>(make_double2(y.x - (P[q][0][0] - qp0), y.y - (pp0 + Q[q][0][0])));
+          }
+          if (t0 + 1 < S) {
+            const double2 y = to_d(yb[(t0 + 1) * us + e]);
+            zb[(t0 + 1) * us + e] = from_d<T>(make_double2(y.x - (P[q][0][1] - qp1), y.y - (pp1 + Q[q][0][1])));
+          }
         }
-        if (t0 + 1 < S) {
-          const double2 y = to_d(yb[(t0 + 1) * us + e]);
-          zb[(t0 + 1) * us + e] = from_d<T>(make_double2(y.x - (P[q][1] - qp1), y.y - (pp1 + Q[q][1])));
+      } else if (ein) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int t = 2 * tig + i;
+          if (t < S) {
+            const double2 y = to_d(yb[t * us + e]);
+            zb[t * us + e] = from_d<T>(make_double2(y.x - (P[q][0][i] - Q[q][NT - 1][i]),
+                                                    y.y - (P[q][NT - 1][i] + Q[q][0][i])));
+          }
         }
       }
     }

@@ -80,7 +80,7 @@ typedef struct {
   double reltol;        /* solver.tolerance (convergent_born.jl:744) */
   double abstol;        /* solver.tolerance * 1e-2 (convergent_born.jl:745) */
   double timeout_s;     /* host-side deadline for the whole call, 0 = none */
-  int block;            /* FM_ORTHO_BLOCK: vectors per block, 2..5 (0: 4); ignored otherwise */
+  int block;            /* FM_ORTHO_BLOCK: vectors per block, 2..8 (0: 4); ignored otherwise */
   int block_store;      /* FM_ORTHO_BLOCK: FM_BLOCK_FP64 or FM_BLOCK_STORAGE; ignored otherwise */
 } fm_solve_opts;
 

@@ -31,7 +31,8 @@ def _solve(grid, radius, precision, block, tol=1e-6, sources=None, store="fp64")
 
 
 @pytest.mark.parametrize("precision,block", [("float64", 2), ("float64", 3), ("float64", 4), ("float64", 5),
-                                             ("float32-math64", 3), ("float32-math64", 4), ("float32-math64", 5),
+                                             ("float64", 6), ("float64", 8), ("float32-math64", 3),
+                                             ("float32-math64", 4), ("float32-math64", 5), ("float32-math64", 6),
                                              ("float32", 4)])
 def test_block_gmres_matches_oracle(precision, block):
     """100 non-converged iterations (the reference's iteration limit on this case)."""
@@ -84,7 +85,7 @@ def test_block_gmres_oblique_fp32_math64(store):
 
 def test_block_gmres_rejects_restart_and_bad_sizes():
     grid = (16, 16, 8)
-    for ls in (F.KrylovJL_GMRES(ortho="block", gmres_restart=10), F.KrylovJL_GMRES(ortho="block", block_size=7)):
+    for ls in (F.KrylovJL_GMRES(ortho="block", gmres_restart=10), F.KrylovJL_GMRES(ortho="block", block_size=9)):
         ocfg, solver = configs(grid, absorbing_z(8), linear_solver=ls)
         with pytest.raises((ValueError, F._lib.FMError)):
             F.solve(solver, xpol()[1], F.Medium(bead(grid, 2.0), EPS_BG))
