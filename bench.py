@@ -208,6 +208,11 @@ def run(args):
                                     linear_solver=F.KrylovJL_GMRES(ortho=args.ortho, block_size=args.block,
                                                                    block_vectors=args.block_store),
                                     max_rhs=args.nrhs, device_index=dev)
+    tuning = None
+    if args.autotune:
+        from fmcuda import autotune as AT
+        tuning = AT.autotune(solver, lists, med)
+        AT.configure(solver, tuning)
     plan = solver.plan()
     info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
     opts = solver.solve_options(int(info.bornmax))
@@ -270,6 +275,7 @@ def run(args):
     h2d = g * 16 + sum(GRID[d] + 2 * solver.padding()[d] for d in range(3)) * 8
     d2h = 2 * args.nrhs * 3 * g * 16
 
+    solver.release()  # the batched plan's device memory is not needed past this point
     # plain FP64 GPU method (reference algorithm: GMRES with MGS, one RHS) and accuracy vs it
     fp64 = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
                                   precision="float64", linear_solver=F.KrylovJL_GMRES(ortho="mgs"), max_rhs=1,
@@ -319,7 +325,6 @@ def run(args):
                    "GBps": round(v["bytes"] / (v["ms"] / 1000) / 1e9, 1) if v["ms"] > 0 else None}
                for k, v in kstats.items() if v["launches"]}
 
-    solver.release()
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args)
@@ -338,7 +343,8 @@ def run(args):
                                         + (", FP64 FFT/Green/V arithmetic" if args.precision != "float32" else ""),
                            "ortho": args.ortho + (f"-{args.block}-{args.block_store}" if args.ortho == "block" else ""),
                            "parallelism": f"replicas{world}",
-                           "l2": "inputs larger than L2 (Krylov basis of 50 MB vectors)", "seed": SEED},
+                           "l2": "inputs larger than L2 (Krylov basis of 50 MB vectors)", "seed": SEED,
+                           "tuning": tuning},
                 "latency_s": {"p50": statistics.median(times), "p99": float(np.percentile(times, 99)),
                               "unit": "batched step"},
                 "iterations": {"min": min(iters), "max": max(iters)},
@@ -412,6 +418,7 @@ def main():
     ap.add_argument("--block-store", default="fp64", choices=["fp64", "storage"],
                     help="raw block vectors in complex FP64 or in the plan's storage type")
     ap.add_argument("--accuracy-rhs", type=int, default=8, help="right-hand sides checked against plain FP64")
+    ap.add_argument("--autotune", type=int, default=1, help="1: pick launch shapes and block size with fmcuda.autotune")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=3)

@@ -84,6 +84,8 @@ struct fm_plan {
   cudaStream_t st = nullptr;
   int sms = 148;
   bool use_tma = true;  // TMA-staged y/z passes (FMCUDA_NO_TMA=1 selects the register-only passes)
+  bool tma_y = true, tma_z = true;  // tuning: TMA-staged y / z passes where the size has one
+  int wave_rhs = 0;                 // tuning: right-hand sides per wave at most (0: as many as memory holds)
   DevBuf errbuf;        // device error code written by bounded pipeline waits
   bool avg = false;     // any absorbing axis
   bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
@@ -190,7 +192,7 @@ static cudaError_t pass_xf(const fm_plan* P, const Dims& d, int pro, const void*
 template <typename S>
 static cudaError_t pass_y(const fm_plan* P, const Dims& d, int dir, const void* in, const void* tw, const void* ramp,
                           void* out, const int* act) {
-  if (P->use_tma && !ramp) {
+  if (P->use_tma && P->tma_y && !ramp) {
     cudaError_t e;
     if constexpr (std::is_same<S, double>::value)
       e = launch_y_tma<double, double>(d, dir, in, tw, ramp, out, act, (int*)P->errbuf.p, P->sms, P->st);
@@ -206,7 +208,7 @@ static cudaError_t pass_y(const fm_plan* P, const Dims& d, int dir, const void* 
 template <typename S>
 static cudaError_t pass_zg(const fm_plan* P, const Dims& d, int mode, const void* in, const GreenParams& gp,
                            const void* tw, const void* rz, void* out, const int* act) {
-  if (P->use_tma) {
+  if (P->use_tma && P->tma_z) {
     cudaError_t e;
     if constexpr (std::is_same<S, double>::value)
       e = launch_zg_tma<double, double>(d, mode, in, gp, tw, rz, out, act, (int*)P->errbuf.p, P->sms, P->st);
@@ -1603,6 +1605,7 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   const size_t avail = (size_t)((freeb + held) * 0.92);
   wave = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, avail / per));
   wave = std::min(wave, std::max(1, P->desc.max_rhs));
+  if (P->wave_rhs > 0) wave = std::min(wave, P->wave_rhs);
   // balance the waves: ceil(nrhs / waves) right-hand sides each
   const int waves = (nrhs + wave - 1) / wave;
   wave = (nrhs + waves - 1) / waves;
@@ -2133,6 +2136,45 @@ int fm_kernel_stats(fm_plan* P, fm_kernel_stat* out, int max) {
 long long fm_launch_count(fm_plan* P) { return P ? P->total_launches : -1; }
 
 void* fm_stream(fm_plan* P) { return P ? (void*)P->st : nullptr; }
+
+fm_status fm_plan_set_tuning(fm_plan* P, int knob, int value) {
+  if (!P) return fail(FM_ERR_INVALID, "null plan");
+  FM_CK(cudaSetDevice(P->desc.device));
+  FM_CK(cudaStreamSynchronize(P->st));
+  switch (knob) {
+    case FM_TUNE_Y_TMA:
+    case FM_TUNE_Z_TMA:
+      if (value != 0 && value != 1) return fail(FM_ERR_INVALID, "TMA tuning value must be 0 or 1");
+      (knob == FM_TUNE_Y_TMA ? P->tma_y : P->tma_z) = value != 0;
+      return FM_OK;
+    case FM_TUNE_TMA_CTAS_PER_SM:
+      if (value < 0 || value > 32) return fail(FM_ERR_INVALID, "TMA CTAs per SM must be 0..32");
+      P->dims.tma_ctas = value;
+      return FM_OK;
+    case FM_TUNE_ROW_THREADS:
+      if (value != 128 && value != 256) return fail(FM_ERR_INVALID, "row-pass threads must be 128 or 256");
+      P->dims.row_threads = value;
+      return FM_OK;
+    case FM_TUNE_WAVE_RHS:
+      if (value < 0) return fail(FM_ERR_INVALID, "right-hand sides per wave must be >= 0");
+      P->wave_rhs = value;
+      return FM_OK;
+    default:
+      return fail(FM_ERR_INVALID, "unknown tuning knob");
+  }
+}
+
+fm_status fm_plan_get_tuning(fm_plan* P, int knob, int* value) {
+  if (!P || !value) return fail(FM_ERR_INVALID, "null argument");
+  switch (knob) {
+    case FM_TUNE_Y_TMA: *value = P->tma_y ? 1 : 0; return FM_OK;
+    case FM_TUNE_Z_TMA: *value = P->tma_z ? 1 : 0; return FM_OK;
+    case FM_TUNE_TMA_CTAS_PER_SM: *value = P->dims.tma_ctas; return FM_OK;
+    case FM_TUNE_ROW_THREADS: *value = P->dims.row_threads; return FM_OK;
+    case FM_TUNE_WAVE_RHS: *value = P->wave_rhs; return FM_OK;
+    default: return fail(FM_ERR_INVALID, "unknown tuning knob");
+  }
+}
 
 // ===========================================================================
 // Slot engine: continuous batching of independent right-hand sides.

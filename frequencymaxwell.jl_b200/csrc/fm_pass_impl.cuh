@@ -10,8 +10,10 @@ static void allow_smem(K kern, size_t bytes) {
   if (bytes > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-constexpr int ROW_THREADS = 256;
+constexpr int ROW_THREADS = 256;  // default threads per block of the row passes
 constexpr int ZG_THREADS = 128;
+// threads per block of the x and y row passes: 128 or 256 (the tuning value in Dims), else the default
+static inline int row_threads(const Dims& d) { return d.row_threads == 128 ? 128 : ROW_THREADS; }
 
 template <typename S, typename R, int L, int PRO>
 static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const double* rs, const void* tw, const void* ramp,
@@ -19,13 +21,14 @@ static cudaError_t xf_L(const Dims& d, const void* in, const void* V, const doub
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
-  constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
+  constexpr int PW = 32 / P_::TP;
+  const int W = row_threads(d) / 32;
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xf<S, R, L, PRO>, smem);
-  k_xf<S, R, L, PRO><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, rs, (const T*)tw,
+  k_xf<S, R, L, PRO><<<blocks, W * 32, smem, st>>>(d, (const TS*)in, (const TS*)V, rs, (const T*)tw,
                                                          (const T*)ramp, (TS*)out, act, vt);
   return cudaGetLastError();
 }
@@ -37,13 +40,14 @@ static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
-  constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
+  constexpr int PW = 32 / P_::TP;
+  const int W = row_threads(d) / 32;
   const long long rows = (long long)d.ny * d.nz * d.nb;
   const long long warps = rows / PW;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
   allow_smem(k_xi<S, R, L, EPI>, smem);
-  k_xi<S, R, L, EPI><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, (const TS*)bv,
+  k_xi<S, R, L, EPI><<<blocks, W * 32, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, (const TS*)bv,
                                                          rs, ep, (const T*)tw, (const T*)ramp, (TS*)out, act, vt);
   return cudaGetLastError();
 }
@@ -54,12 +58,13 @@ static cudaError_t y_L(const Dims& d, const void* in, const void* tw, const void
   using T = cplx<R>;
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
-  constexpr int PW = 32 / P_::TP, W = ROW_THREADS / 32;
+  constexpr int PW = 32 / P_::TP;
+  const int W = row_threads(d) / 32;
   const long long warps = (long long)(d.nx / PW) * d.nz * 3 * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, false>::v) * sizeof(T);
   allow_smem(k_y<S, R, L, DIR>, smem);
-  k_y<S, R, L, DIR><<<blocks, ROW_THREADS, smem, st>>>(d, (const TS*)in, (const T*)tw, (const T*)ramp, (TS*)out, act);
+  k_y<S, R, L, DIR><<<blocks, W * 32, smem, st>>>(d, (const TS*)in, (const T*)tw, (const T*)ramp, (TS*)out, act);
   return cudaGetLastError();
 }
 
@@ -216,9 +221,10 @@ static bool make_map(CUtensorMap* m, void* base, const Dims& d, int esz, int ran
 }
 
 template <typename K>
-static unsigned persistent_grid(K kern, int threads, size_t smem, long long ntiles, int sms) {
+static unsigned persistent_grid(K kern, int threads, size_t smem, long long ntiles, int sms, int cap = 0) {
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem) != cudaSuccess || bps < 1) bps = 1;
+  if (cap > 0 && bps > cap) bps = cap;  // tuning: fewer persistent CTAs per SM
   long long g = (long long)sms * bps;
   if (g > ntiles) g = ntiles;
   return (unsigned)(g < 1 ? 1 : g);
@@ -237,7 +243,7 @@ static cudaError_t y_tma_L(const Dims& d, const void* in, const void* tw, const 
   const size_t smem = C::SM::total;
   allow_smem(k_y_tma<S, R, L, DIR>, smem);
   const long long ntiles = (long long)(d.nx / C::TX) * d.nz * 3 * d.nb;
-  const unsigned grid = persistent_grid(k_y_tma<S, R, L, DIR>, C::THREADS, smem, ntiles, sms);
+  const unsigned grid = persistent_grid(k_y_tma<S, R, L, DIR>, C::THREADS, smem, ntiles, sms, d.tma_ctas);
   k_y_tma<S, R, L, DIR><<<grid, C::THREADS, smem, st>>>(d, mi, mo, (const cplx<R>*)tw + 0, (const cplx<R>*)ramp, act,
                                                          err);
   return cudaGetLastError();
@@ -255,7 +261,7 @@ static cudaError_t zg_tma_L(const Dims& d, const void* in, const GreenParams& gp
   const size_t smem = C::SM::total;
   allow_smem(k_zg_tma<S, R, L, MODE>, smem);
   const long long ntiles = (long long)(d.nx / C::TX) * d.ny * d.nb;
-  const unsigned grid = persistent_grid(k_zg_tma<S, R, L, MODE>, C::THREADS, smem, ntiles, sms);
+  const unsigned grid = persistent_grid(k_zg_tma<S, R, L, MODE>, C::THREADS, smem, ntiles, sms, d.tma_ctas);
   k_zg_tma<S, R, L, MODE><<<grid, C::THREADS, smem, st>>>(d, mi, mo, gp, (const cplx<R>*)tw, (const cplx<R>*)rz, act,
                                                            err);
   return cudaGetLastError();

@@ -28,6 +28,8 @@ struct Dims {
   int nx, ny, nz, nb;
   long long n;           // nx*ny*nz
   long long vstride = 0; // potential of RHS b at V + b*vstride (0: one potential shared by all RHS)
+  int row_threads = 256; // launch shape (tuning): threads per block of the x and y row passes (128 or 256)
+  int tma_ctas = 0;      // launch shape (tuning): persistent CTAs per SM of the TMA passes (0: occupancy limit)
 };
 
 // Optional per-RHS vector pointers (RHS b's field starts at tab[b]); null -> contiguous batch.

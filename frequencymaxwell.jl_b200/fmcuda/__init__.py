@@ -14,6 +14,6 @@ from .solver import (BornSeries, ConvergentBornSolver, DevicePlan, KrylovJL_BICG
                      domain_size, grid_spacing, reset, solve, solve_batch)
 from .sources import (AbstractCurrentSource, PlaneWaveSource, generate_incident_field, illumination_cone,
                       source_wavelength)
-from . import _lib
+from . import _lib, autotune as autotuner
 
 __all__ = [n for n in dir() if not n.startswith("_")]

@@ -19,6 +19,7 @@ FM_PREC_F64, FM_PREC_F32, FM_PREC_F32_MATH64 = 0, 1, 2
 FM_METHOD_GMRES, FM_METHOD_BICGSTAB, FM_METHOD_RICHARDSON = 0, 1, 2
 FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2, FM_ORTHO_BLOCK = 0, 1, 2, 3
 FM_BLOCK_FP64, FM_BLOCK_STORAGE = 0, 1
+FM_TUNE_Y_TMA, FM_TUNE_Z_TMA, FM_TUNE_TMA_CTAS_PER_SM, FM_TUNE_ROW_THREADS, FM_TUNE_WAVE_RHS = 0, 1, 2, 3, 4
 
 STATUS_NAMES = {
     FM_OK: "FM_OK", FM_ERR_INVALID: "FM_ERR_INVALID", FM_ERR_OOM: "FM_ERR_OOM",
@@ -33,7 +34,7 @@ EXPORTED = (
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
     "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream", "fm_green_apply_noalloc",
     "fm_engine_slot_bytes", "fm_engine_create", "fm_engine_destroy", "fm_engine_submit", "fm_engine_step",
-    "fm_engine_status",
+    "fm_engine_status", "fm_plan_set_tuning", "fm_plan_get_tuning",
 )
 
 
@@ -110,6 +111,10 @@ def lib() -> C.CDLL:
     L.fm_kernel_stats.restype = C.c_int
     L.fm_launch_count.argtypes = [P]
     L.fm_launch_count.restype = C.c_longlong
+    L.fm_plan_set_tuning.argtypes = [P, C.c_int, C.c_int]
+    L.fm_plan_set_tuning.restype = C.c_int
+    L.fm_plan_get_tuning.argtypes = [P, C.c_int, C.POINTER(C.c_int)]
+    L.fm_plan_get_tuning.restype = C.c_int
     L.fm_engine_slot_bytes.argtypes = [C.POINTER(fm_plan_desc), C.c_int]
     L.fm_engine_slot_bytes.restype = C.c_longlong
     L.fm_engine_create.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, P, P, P, C.c_int, C.POINTER(P)]

@@ -66,12 +66,14 @@ class ConvergentBornSolver:
     ``precision`` ("float64" / "float32" / "float32-math64": FP32 fields in HBM with FP64 arithmetic in the
     FFT, Green and potential kernels) replaces Julia's element-type parameter T; by default it is
     float32 when ``resolution`` holds numpy float32 values and float64 otherwise (the reference promotes
-    the type of resolution and tolerance).  ``max_rhs`` bounds the batch held on the device at once."""
+    the type of resolution and tolerance).  ``max_rhs`` bounds the batch held on the device at once.
+    ``autotune=True`` picks launch shapes and the batch schedule for each batch shape on first use
+    (fmcuda.autotune; cached on disk)."""
 
     def __init__(self, resolution: Sequence[float], grid_size: Sequence[int], boundary_conditions,
                  iterations_max: int = -1, tolerance: float = 1e-6, linear_solver=None,
                  preconditioner: str = "none", device: str = "fmcuda", precision: Optional[str] = None,
-                 max_rhs: int = 64, device_index: int = 0):
+                 max_rhs: int = 64, device_index: int = 0, autotune: bool = False):
         if precision is None:
             precision = "float32" if all(isinstance(r, np.float32) for r in resolution) else "float64"
         if precision not in ("float32", "float64", "float32-math64"):
@@ -100,6 +102,7 @@ class ConvergentBornSolver:
         self.precision = precision
         self.max_rhs = int(max_rhs)
         self.device_index = int(device_index)
+        self.autotune = bool(autotune)
         self.backend = "fmcuda"
         self.Green_function = None
         self.Bornmax = 0
@@ -394,6 +397,9 @@ def solve_batch(solver: ConvergentBornSolver, sources_list: Sequence, medium: Me
     for s in lists:
         if source_wavelength(s) != wl:
             raise ValueError("all right-hand sides must share the wavelength of the potential")
+    if solver.autotune:
+        from . import autotune as AT
+        AT.configure(solver, AT.autotune(solver, lists, medium))
     plan, _ = _prepare(solver, medium, wl)
     E, H, infos, st = plan.solve_plane_waves(lists, medium.permittivity_bg, solver.solve_options(solver.Bornmax))
     _record(solver, infos, st)

@@ -231,6 +231,17 @@ long long fm_launch_count(fm_plan* plan);
 /* The plan's cudaStream_t, for callers that time work on it with their own events. */
 void* fm_stream(fm_plan* plan);
 
+/* Launch-shape and batch-schedule knobs of a plan, set by the autotuner (fmcuda/autotune.py).  They change
+ * how work is launched, never what is computed.  No counterpart in the reference.
+ *   FM_TUNE_Y_TMA, FM_TUNE_Z_TMA    1: TMA-staged y / z passes where the axis length has one, 0: register-only
+ *   FM_TUNE_TMA_CTAS_PER_SM         persistent CTAs per SM of the TMA passes, 0 = occupancy limit
+ *   FM_TUNE_ROW_THREADS             threads per block of the x and y row passes: 128 or 256
+ *   FM_TUNE_WAVE_RHS                right-hand sides per wave at most, 0 = as many as device memory holds */
+enum { FM_TUNE_Y_TMA = 0, FM_TUNE_Z_TMA = 1, FM_TUNE_TMA_CTAS_PER_SM = 2, FM_TUNE_ROW_THREADS = 3,
+       FM_TUNE_WAVE_RHS = 4 };
+fm_status fm_plan_set_tuning(fm_plan* plan, int knob, int value);
+fm_status fm_plan_get_tuning(fm_plan* plan, int knob, int* value);
+
 #ifdef __cplusplus
 }
 #endif
