@@ -315,6 +315,14 @@ def run(args):
     achieved = ds["bytes"] / (ds["ms"] / 1000.0) / 1e9 if ds["ms"] > 0 else 0.0
     total_ms = sum(v["ms"] for v in kstats.values())
     traffic = None
+    try:  # DRAM / algorithmic bytes of this kernel class from its ncu capture (profiles/traffic.txt)
+        with open(os.path.join(ROOT, "profiles", "traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if parts and not line.startswith("#") and parts[0] == dname:
+                    traffic = float(parts[1]) * ds["bytes"] / max(1, ds["launches"])
+    except OSError:
+        pass
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": dname, "peak_kind": peak_kind,
             "share": ds["ms"] / total_ms if total_ms > 0 else None,
