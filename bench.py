@@ -393,6 +393,54 @@ def run_serving(args):
     return rep
 
 
+def run_large(args):
+    """The large single configuration: 512x512x256 at 50 nm (padded z 512, the two shifted z branches as two
+    z passes), 40 seeded beads (radius U[6,24] px, index U[1.4,2.0]) in water, 500 nm x-pol +z, GMRES(20) on
+    the CBS-preconditioned operator with FP32 fields and FP64 dots, tolerance 1e-6.  One solve is timed on the
+    device (2-iteration warm-up for the plan and tables)."""
+    import torch
+    import fmcuda as F
+    grid = (512, 512, 256)
+    med = F.phantom_random_beads(grid, 40, (6, 24), (1.4, 2.0), EPS_BG, SEED + 4)
+    bc_z = F.AbsorbingBoundaryCondition(thickness=grid[2] * RES[2], attenuation_thickness=grid[2] * RES[2],
+                                        sharpness=1.0, profile=F.TanhProfile)
+    bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
+    src = F.PlaneWaveSource(wavelength=WL, polarization=[1, 0, 0], k_vector=[0, 0, 1])
+    solver = F.ConvergentBornSolver(resolution=RES, grid_size=grid, boundary_conditions=bcs, tolerance=1e-6,
+                                    precision=args.precision, max_rhs=1,
+                                    linear_solver=F.KrylovJL_GMRES(ortho="cgs", gmres_restart=20))
+    plan = solver.plan()
+    info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
+    opts = solver.solve_options(int(info.bornmax))
+    stream = torch.cuda.ExternalStream(plan.stream(), device=torch.device("cuda", 0))
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        warm = solver.solve_options(int(info.bornmax))
+        warm.maxiters = 2
+        plan.solve_plane_waves([[src]], EPS_BG, warm, keep_on_device=True)
+        plan.set_profiling(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        _, _, infos, st = plan.solve_plane_waves([[src]], EPS_BG, opts, keep_on_device=True)
+        ev1.record(stream)
+        ev1.synchronize()
+    t = ev0.elapsed_time(ev1) / 1000.0
+    ks = plan.kernel_stats()
+    plan.set_profiling(False)
+    tot = sum(v["ms"] for v in ks.values())
+    out = {"workload": "large single: 512x512x256 (padded 512^3), 40 beads n 1.4-2.0, GMRES(20), tol 1e-6",
+           "precision": args.precision, "bornmax": int(info.bornmax), "maxiters": int(opts.maxiters),
+           "iterations": int(infos[0].iterations), "solved": bool(infos[0].solved),
+           "relative_residual": float(infos[0].residual / infos[0].residual0), "seconds_per_solve": t,
+           "born_iterations_per_s": infos[0].iterations / t,
+           "kernel_classes": {k: {"ms": round(v["ms"], 1), "GBps": round(v["bytes"] / (v["ms"] / 1000) / 1e9, 1)}
+                              for k, v in ks.items() if v["launches"] and v["ms"] > 0},
+           "share_top": max(((k, v["ms"] / tot) for k, v in ks.items()), key=lambda kv: kv[1]) if tot else None}
+    solver.release()
+    return out
+
+
 def run_operator_case(args):
     """Small case for profilers: `reps` applications of the CBS operator on `nrhs` seeded random fields
     on the bench grid (no solve)."""
@@ -438,11 +486,15 @@ def main():
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
     ap.add_argument("--serving-basis", type=int, default=100)
     ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
+    ap.add_argument("--large-only", action="store_true", help="run the large single configuration and print it")
     args = ap.parse_args()
     if args.operator_case:
         return run_operator_case(args)
     if args.serving_only:
         print(json.dumps({"serving": run_serving(args)}))
+        return 0
+    if args.large_only:
+        print(json.dumps({"large": run_large(args)}))
         return 0
     if args.impl == "reference":
         return run_reference(args)

@@ -89,6 +89,7 @@ struct fm_plan {
   DevBuf errbuf;        // device error code written by bounded pipeline waits
   bool avg = false;     // any absorbing axis
   bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
+  bool zsplit = false;  // shifts only on z, padded z longer than the length-2L pass takes: two z passes
   double shift[3] = {0, 0, 0};
   // potential / physics
   bool have_pot = false;
@@ -254,6 +255,9 @@ static fm_status init_tables(fm_plan* P) {
   if (P->zonly) {
     FM_CK(upload_cplx<R>(P->twz2, twiddles<R>(2 * P->dims.nz), P->st));
     FM_CK(upload_cplx<R>(P->rz, ramp(P->dims.nz, P->shift[2], -1.0), P->st));
+  } else if (P->zsplit) {
+    FM_CK(upload_cplx<R>(P->rzp, ramp(P->dims.nz, P->shift[2], -1.0), P->st));
+    FM_CK(upload_cplx<R>(P->rzm, ramp(P->dims.nz, P->shift[2], +1.0), P->st));
   } else if (P->avg) {
     FM_CK(upload_cplx<R>(P->rxp, ramp(P->dims.nx, P->shift[0], -1.0), P->st));
     FM_CK(upload_cplx<R>(P->rxm, ramp(P->dims.nx, P->shift[0], +1.0), P->st));
@@ -361,6 +365,29 @@ static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const dou
     FM_TRACK(P, KC_ZG, 2 * fbA,
              e = pass_zg<R>(P, d, mode, P->t2.p, gp, P->zonly ? P->twz2.p : P->twz.p, P->zonly ? P->rz.p : nullptr,
                               P->t1.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_YI, 2 * fbA, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
+    FM_CK(e);
+    FM_TRACK(P, KC_XI, xib, e = pass_xi<R>(P, d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act, vt));
+    FM_CK(e);
+    return FM_OK;
+  }
+  if (P->zsplit) {
+    // the two z branches (+s, -s) as two length-L z passes with their phase ramps; the second adds to the first
+    gp.scale_re = 1.0 / ((double)P->n * 2.0);
+    cudaError_t e;
+    FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
+             e = pass_xf<R>(P, d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act, vt));
+    FM_CK(e);
+    FM_TRACK(P, KC_YF, 2 * fbA, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
+    FM_CK(e);
+    gp.shift[2] = P->shift[2];
+    gp.accumulate = 0;
+    FM_TRACK(P, KC_ZG, 2 * fbA, e = pass_zg<R>(P, d, ZMODE_ONE, P->t2.p, gp, P->twz.p, P->rzp.p, P->t1.p, act));
+    FM_CK(e);
+    gp.shift[2] = -P->shift[2];
+    gp.accumulate = 1;
+    FM_TRACK(P, KC_ZG, 3 * fbA, e = pass_zg<R>(P, d, ZMODE_ONE, P->t2.p, gp, P->twz.p, P->rzm.p, P->t1.p, act));
     FM_CK(e);
     FM_TRACK(P, KC_YI, 2 * fbA, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
     FM_CK(e);
@@ -1654,14 +1681,16 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   bool avg = desc->absorbing[0] || desc->absorbing[1] || desc->absorbing[2];
   bool zonly = desc->absorbing[2] && !desc->absorbing[0] && !desc->absorbing[1];
   if (avg && !zonly) return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build");
-  if (zonly && (n3[2] > AXIS_MAX_AVG2 || (n3[2] & (n3[2] - 1))))
+  if (zonly && (n3[2] > AXIS_MAX || (n3[2] & (n3[2] - 1))))
     return fail(FM_ERR_UNSUPPORTED,
-                "an absorbing z boundary needs a power-of-two padded z size of at most 256 in this build");
+                "an absorbing z boundary needs a power-of-two padded z size of at most 512 in this build");
+  // padded z above 256: the two shifted branches run as two z passes (the second adds to the first)
+  const bool zsplit = zonly && n3[2] > AXIS_MAX_AVG2;
   const int prec = desc->precision == FM_PREC_F64 ? FM_PREC_F64 : FM_PREC_F32;  // storage
   const bool c64 = desc->precision != FM_PREC_F32;                                   // arithmetic
   const int pwy = c64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
-  const int pwz = c64 ? pencils_per_warp<double>(zonly ? 2 * n3[2] : n3[2])
-                      : pencils_per_warp<float>(zonly ? 2 * n3[2] : n3[2]);
+  const int lz = (zonly && !zsplit) ? 2 * n3[2] : n3[2];
+  const int pwz = c64 ? pencils_per_warp<double>(lz) : pencils_per_warp<float>(lz);
   if (pwy <= 0 || pwz <= 0 || n3[0] % pwy || n3[0] % pwz) return fail(FM_ERR_UNSUPPORTED, "x size too small for pencil tiling");
   if (cudaSetDevice(desc->device) != cudaSuccess) return fail(FM_ERR_CUDA, "cudaSetDevice failed");
   fm_plan* P = new fm_plan();
@@ -1675,7 +1704,8 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   P->M = 3 * P->n;
   P->pi = PadInfo{desc->grid[0], desc->grid[1], desc->grid[2], desc->pad[0], desc->pad[1], desc->pad[2], n3[0], n3[1], n3[2]};
   P->avg = avg;
-  P->zonly = zonly;
+  P->zonly = zonly && !zsplit;
+  P->zsplit = zsplit;
   for (int a = 0; a < 3; ++a) P->shift[a] = desc->absorbing[a] ? 0.25 : 0.0;
   {
     cudaDeviceProp prop;

@@ -188,6 +188,7 @@ struct GreenParams {
   double scale_re, scale_im;  // folded normalisation (and curl factor)
   int curl_index;    // 1 -> curl index formula for odd sizes
   const double* ksq_im_b = nullptr;  // per-RHS imaginary part of k_square (null: ksq_im for all)
+  int accumulate = 0;                // 1: add the result to out (second branch of a split average)
 };
 
 template <typename R>
@@ -311,7 +312,9 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
       if (MODE != ZMODE_AVG2 || z < L) {
         T a = v[c][e];
         if (MODE != ZMODE_CURL && rz) a = cmul(a, cconj(rtab[z]));
-        out[base0 + (long long)c * d.n + (long long)z * plane] = cv<TS>(a);
+        const long long o = base0 + (long long)c * d.n + (long long)z * plane;
+        if (gp.accumulate) a = cadd(a, cv<T>(out[o]));
+        out[o] = cv<TS>(a);
       }
     }
   }
