@@ -250,13 +250,10 @@ def run(args):
     kstats = plan.kernel_stats()
     plan.set_profiling(False)
     t_step = max(times)
-    if dist:
-        t = torch.tensor([statistics.median(times)], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_med = float(t.item())
-    else:
-        t_med = statistics.median(times)
+    from fmcuda.replicas import max_over_ranks
+    t_med = max_over_ranks(statistics.median(times))  # the slowest replica sets the job time
     value = world * args.nrhs / t_med
+    n_pad = float(np.prod(solver.padded_size()))
     iters = [i.iterations for i in infos]
 
     # end to end through the public API (host permittivity in, host E/H out)
@@ -356,6 +353,10 @@ def run(args):
                 "latency_s": {"p50": statistics.median(times), "p99": float(np.percentile(times, 99)),
                               "unit": "batched step"},
                 "iterations": {"min": min(iters), "max": max(iters)},
+                "born_iterations_per_s": world * sum(iters) / t_med,
+                "flops_model": {"per_iteration": 12 * 5 * n_pad * math.log2(n_pad),
+                                "achieved_GFLOPs": world * sum(iters) / t_med * 12 * 5 * n_pad * math.log2(n_pad) / 1e9,
+                                "model": "12 x 5 N log2 N per Born iteration (2 branches x fwd+inv x 3 components)"},
                 "fp64_plain": {"solves_per_s": fp64_sps, "iterations": fp64_iters,
                                "rel_l2_E_fp32_vs_fp64": err_e, "rel_l2_H_fp32_vs_fp64": err_h,
                                "rel_l2_over_rhs": len(errs_e), "bar": 1e-5,
