@@ -439,7 +439,40 @@ def run_large(args):
                               for k, v in ks.items() if v["launches"] and v["ms"] > 0},
            "share_top": max(((k, v["ms"] / tot) for k, v in ks.items()), key=lambda kv: kv[1]) if tot else None}
     solver.release()
+    if args.large_check:
+        out["fp32_vs_fp64_check"] = large_check(args)
     return out
+
+
+def large_check(args):
+    """The large configuration's accuracy check at reduced lateral size: 128x128x256 (the same padded z of 512,
+    two shifted z passes), 10 beads with the large configuration's statistics (radius U[6,24] px, index
+    U[1.4,2.0]), x-pol +z, GMRES(20).  The FP32-field form against the plain FP64 GPU method (MGS), both full
+    solves; the full 512^3 FP64 solve needs ~182 GB and does not fit one GPU."""
+    import fmcuda as F
+    grid = (128, 128, 256)
+    med = F.phantom_random_beads(grid, 10, (6, 24), (1.4, 2.0), EPS_BG, SEED + 5)
+    bc_z = F.AbsorbingBoundaryCondition(thickness=grid[2] * RES[2], attenuation_thickness=grid[2] * RES[2],
+                                        sharpness=1.0, profile=F.TanhProfile)
+    bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
+    src = F.PlaneWaveSource(wavelength=WL, polarization=[1, 0, 0], k_vector=[0, 0, 1])
+    res = {}
+    for prec, ortho in ((args.precision, "cgs"), ("float64", "mgs")):
+        sv = F.ConvergentBornSolver(resolution=RES, grid_size=grid, boundary_conditions=bcs, tolerance=1e-6,
+                                    precision=prec, max_rhs=1, linear_solver=F.KrylovJL_GMRES(ortho=ortho,
+                                                                                            gmres_restart=20))
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            t0 = time.perf_counter()
+            f = F.solve(sv, src, med)
+            dt = time.perf_counter() - t0
+        res[prec] = (f, sv.iteration_count, sv.residual_history[-1], dt)
+        sv.release()
+    f32, it32, r32, t32 = res[args.precision]
+    f64, it64, r64, t64 = res["float64"]
+    return {"grid": list(grid), "padded_z": 512, "iterations": [it32, it64], "seconds": [t32, t64],
+            "rel_l2_E": rel_l2(f32.E, f64.E), "rel_l2_H": rel_l2(f32.H, f64.H),
+            "residual_ratio": r32 / r64 if r64 else None}
 
 
 def run_operator_case(args):
@@ -488,6 +521,7 @@ def main():
     ap.add_argument("--serving-basis", type=int, default=100)
     ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
     ap.add_argument("--large-only", action="store_true", help="run the large single configuration and print it")
+    ap.add_argument("--large-check", type=int, default=1, help="with --large-only: FP32 vs FP64 check at 128x128x256")
     args = ap.parse_args()
     if args.operator_case:
         return run_operator_case(args)
