@@ -213,6 +213,9 @@ def run(args):
         from fmcuda import autotune as AT
         tuning = AT.autotune(solver, lists, med)
         AT.configure(solver, tuning)
+    if args.block_dot >= 0:
+        from fmcuda import autotune as AT
+        AT.apply(solver.plan(), {"block_dot": args.block_dot})
     plan = solver.plan()
     info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
     opts = solver.solve_options(int(info.bornmax))
@@ -509,6 +512,8 @@ def main():
                     help="raw block vectors in complex FP64 or in the plan's storage type")
     ap.add_argument("--accuracy-rhs", type=int, default=8, help="right-hand sides checked against plain FP64")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick launch shapes and block size with fmcuda.autotune")
+    ap.add_argument("--block-dot", type=int, default=-1,
+                    help="block dot of block GMRES: 1 bulk-copy pipeline, 0 register-staged, -1 the plan's default")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=3)

@@ -5,6 +5,8 @@
 #include <mutex>
 #include <memory>
 #include <deque>
+#include <future>
+#include <thread>
 #include <cstdlib>
 #include <chrono>
 #include <cmath>
@@ -15,6 +17,7 @@
 #include <vector>
 
 #include "../../include/fmcuda.h"
+#include "fm_blockdot.h"
 #include "fm_krylov.cuh"
 #include "fm_launch.h"
 #include "fm_setup.cuh"
@@ -85,6 +88,7 @@ struct fm_plan {
   int sms = 148;
   bool use_tma = true;  // TMA-staged y/z passes (FMCUDA_NO_TMA=1 selects the register-only passes)
   bool tma_y = true, tma_z = true;  // tuning: TMA-staged y / z passes where the size has one
+  bool bd_bulk = false;             // tuning: bulk-copy pipelined block dot where the shape has one
   int wave_rhs = 0;                 // tuning: right-hand sides per wave at most (0: as many as memory holds)
   DevBuf errbuf;        // device error code written by bounded pipeline waits
   bool avg = false;     // any absorbing axis
@@ -105,6 +109,12 @@ struct fm_plan {
   DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
   DevBuf Eo, Ho;
   int out_nrhs = 0;
+  // copies of the output fields to the caller's host buffers (solve_waves_t): a copy stream, a pinned staging
+  // ring of two chunks, "chunk landed" events and "output slot assembled" events
+  cudaStream_t cst = nullptr;
+  void* stage_h = nullptr;
+  cudaEvent_t cev[2] = {nullptr, nullptr};
+  cudaEvent_t ready[2] = {nullptr, nullptr};
   // launch accounting (always) and event timing per kernel class (when prof is on)
   bool prof = false;
   long long launches[16] = {0};
@@ -933,6 +943,19 @@ template <typename R, typename YR, int S>
 static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, const void* Y, const int* act, int nact) {
   using T = cplx<R>;
   using TY = cplx<YR>;
+  const double bytes = ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
+  const size_t pb =
+      P->bd_bulk ? blockdot_bulk_part_bytes((int)sizeof(R), (int)sizeof(YR), S, P->M, nb, nact, K, P->sms) : 0;
+  if (pb) {
+    cudaError_t e = P->red_part.ensure(pb);
+    if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
+    if (e != cudaSuccess) return e;
+    FM_TRACK(P, KC_DOT, bytes,
+             e = launch_blockdot_bulk((int)sizeof(R), (int)sizeof(YR), S, P->M, nb, nact, K, U, Y,
+                                      (double2*)P->red_part.p, P->red_part.cap, (double2*)P->red_out.p,
+                                      (unsigned*)P->red_cnt.p, act, (int*)P->errbuf.p, P->sms, P->st));
+    return e;
+  }
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
       bps < 1)
@@ -942,7 +965,7 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
   cudaError_t e = P->red_part.ensure((size_t)nb * nblk * K * S * sizeof(double2));
   if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
   if (e != cudaSuccess) return e;
-  FM_TRACK(P, KC_DOT, ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M,
+  FM_TRACK(P, KC_DOT, bytes,
            (k_blockdot_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
                P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
                (unsigned*)P->red_cnt.p, act)));
@@ -1626,7 +1649,8 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   else if (o.method == FM_METHOD_BICGSTAB) vecs = 6;
   else vecs = 1;
   // basis + b + x + s + e + t1 + t2 + fp64 staging and outputs
-  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 3 + extra;
+  // (the output term also covers the second output slot of host-output solves: 2 * 3g * 16 <= 2 * M * 16)
+  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 5 + extra;
   const size_t held = P->basis.cap + P->bbuf.cap + P->xbuf.cap + P->sbuf.cap + P->ebuf.cap + P->t1.cap + P->t2.cap +
                       P->gbuf2.cap + P->Eo.cap + P->Ho.cap + P->yblk.cap;
   const size_t avail = (size_t)((freeb + held) * 0.92);
@@ -1740,10 +1764,17 @@ void fm_plan_destroy(fm_plan* P) {
                     &P->rzm, &P->V, &P->t1, &P->t2, &P->bbuf, &P->xbuf, &P->ebuf, &P->sbuf, &P->basis,
                     &P->gbuf2, &P->red_part, &P->red_out, &P->red_cnt, &P->active, &P->scale, &P->coef,
                     &P->hbuf, &P->eps_dev, &P->fx, &P->fy, &P->fz, &P->maxpart, &P->maxout, &P->wt_x,
-                    &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho, &P->errbuf};
+                    &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho, &P->errbuf,
+                    &P->shifts, &P->yblk, &P->V64};
   for (DevBuf* b : bufs) b->release();
   tk_resolve(P);
   for (cudaEvent_t e : P->evpool) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) {
+    if (P->cev[i]) cudaEventDestroy(P->cev[i]);
+    if (P->ready[i]) cudaEventDestroy(P->ready[i]);
+  }
+  if (P->stage_h) cudaFreeHost(P->stage_h);
+  if (P->cst) cudaStreamDestroy(P->cst);
   if (P->st) cudaStreamDestroy(P->st);
   delete P;
 }
@@ -2049,6 +2080,75 @@ static fm_status upload_waves(fm_plan* P, int nrhs, const int* first, const fm_p
   return FM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Output copies.  The caller's E/H buffers are ordinary (pageable) host memory.  A worker thread copies each
+// finished wave device -> pinned staging chunk (copy stream) -> caller buffer (host threads), so the copy of
+// wave i runs while wave i+1 computes, and the host-side page faults of a fresh destination are taken by
+// several threads.  The solve thread's own small reads stay on the compute stream.
+// ---------------------------------------------------------------------------
+constexpr size_t OUT_CHUNK = (size_t)32 << 20;
+
+static fm_status ensure_copier(fm_plan* P) {
+  if (!P->cst) FM_CK(cudaStreamCreateWithFlags(&P->cst, cudaStreamNonBlocking));
+  if (!P->stage_h) FM_CK(cudaHostAlloc(&P->stage_h, 2 * OUT_CHUNK, cudaHostAllocDefault));
+  for (int i = 0; i < 2; ++i) {
+    if (!P->cev[i]) FM_CK(cudaEventCreateWithFlags(&P->cev[i], cudaEventDisableTiming));
+    if (!P->ready[i]) FM_CK(cudaEventCreateWithFlags(&P->ready[i], cudaEventDisableTiming));
+  }
+  return FM_OK;
+}
+
+static void host_copy(char* dst, const char* src, size_t n) {
+  constexpr int NT = 4;
+  if (n < ((size_t)4 << 20)) {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  const size_t part = ((n + NT - 1) / NT + 63) & ~(size_t)63;
+  std::thread th[NT - 1];
+  for (int i = 1; i < NT; ++i) {
+    const size_t a = std::min(n, part * i), b = std::min(n, part * (i + 1));
+    th[i - 1] = std::thread([=] { std::memcpy(dst + a, src + a, b - a); });
+  }
+  std::memcpy(dst, src, std::min(n, part));
+  for (auto& t : th) t.join();
+}
+
+// Copies `bytes` from each of de, dh (device) to E, H (host) once event ready[slot] has completed.
+static cudaError_t copy_out(fm_plan* P, int slot, const void* de, const void* dh, void* E, void* H, size_t bytes) {
+  cudaError_t e = cudaSetDevice(P->desc.device);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(P->cst, P->ready[slot], 0);
+  char* stage = (char*)P->stage_h;
+  char* pdst[2] = {nullptr, nullptr};
+  size_t pn[2] = {0, 0};
+  const char* src[2] = {(const char*)de, (const char*)dh};
+  char* dst[2] = {(char*)E, (char*)H};
+  auto drain = [&](int s) {
+    if (!pdst[s]) return;
+    const cudaError_t e2 = cudaEventSynchronize(P->cev[s]);
+    if (e2 == cudaSuccess) host_copy(pdst[s], stage + s * OUT_CHUNK, pn[s]);
+    else if (e == cudaSuccess) e = e2;
+    pdst[s] = nullptr;
+  };
+  int i = 0;
+  for (int f = 0; f < 2 && e == cudaSuccess; ++f)
+    for (size_t off = 0; off < bytes && e == cudaSuccess; off += OUT_CHUNK, ++i) {
+      const int s = i & 1;
+      drain(s);
+      if (e != cudaSuccess) break;
+      const size_t n = std::min(OUT_CHUNK, bytes - off);
+      e = cudaMemcpyAsync(stage + s * OUT_CHUNK, src[f] + off, n, cudaMemcpyDeviceToHost, P->cst);
+      if (e == cudaSuccess) e = cudaEventRecord(P->cev[s], P->cst);
+      if (e == cudaSuccess) {
+        pdst[s] = dst[f] + off;
+        pn[s] = n;
+      }
+    }
+  drain(i & 1);
+  drain((i + 1) & 1);
+  return e;
+}
+
 template <typename R>
 static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_plane_wave* src, double eps_bg,
                                const fm_solve_opts& o, double* E, double* H, fm_solve_info* info) {
@@ -2056,16 +2156,21 @@ static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_
   FM_TRY(plan_wave_size<R>(P, nrhs, o, wave));
   const long long g = (long long)P->pi.gx * P->pi.gy * P->pi.gz;
   const bool keep = (E == nullptr);
+  // host outputs: two device output slots when there is more than one wave (wave i copied while i+1 runs)
+  const int slots = (!keep && nrhs > wave) ? 2 : 1;
   if (keep) {
     FM_CK(P->Eo.ensure((size_t)nrhs * 3 * g * sizeof(double2)));
     FM_CK(P->Ho.ensure((size_t)nrhs * 3 * g * sizeof(double2)));
   } else {
-    FM_CK(P->Eo.ensure((size_t)wave * 3 * g * sizeof(double2)));
-    FM_CK(P->Ho.ensure((size_t)wave * 3 * g * sizeof(double2)));
+    FM_CK(P->Eo.ensure((size_t)slots * wave * 3 * g * sizeof(double2)));
+    FM_CK(P->Ho.ensure((size_t)slots * wave * 3 * g * sizeof(double2)));
+    FM_TRY(ensure_copier(P));
   }
+  std::future<cudaError_t> pend[2];
   bool all_ok = true;
-  for (int b0 = 0; b0 < nrhs; b0 += wave) {
+  for (int b0 = 0, wi = 0; b0 < nrhs; b0 += wave, ++wi) {
     const int nb = std::min(wave, nrhs - b0);
+    const int slot = wi % slots;
     std::vector<int> f(nb + 1);
     for (int b = 0; b <= nb; ++b) f[b] = first[b0 + b] - first[b0];
     FM_TRY(upload_waves(P, nb, f.data(), src + first[b0], eps_bg));
@@ -2078,15 +2183,19 @@ static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_
     FM_CK(cudaGetLastError());
     std::vector<fm_solve_info> inf(nb);
     FM_TRY(solve_core<R>(P, nb, o, inf));
-    double2* eo = (double2*)P->Eo.p + (keep ? (size_t)b0 * 3 * g : 0);
-    double2* ho = (double2*)P->Ho.p + (keep ? (size_t)b0 * 3 * g : 0);
+    if (pend[slot].valid()) FM_CK(pend[slot].get());  // the slot's previous wave has reached the host
+    const size_t oo = keep ? (size_t)b0 * 3 * g : (size_t)slot * wave * 3 * g;
+    double2* eo = (double2*)P->Eo.p + oo;
+    double2* ho = (double2*)P->Ho.p + oo;
     FM_TRACK(P, KC_SETUP, (double)nb * 3 * g * (2 * sizeof(cplx<R>) + 2 * sizeof(double2)),
              (k_assemble<R><<<dim3(296, nb), 256, 0, P->st>>>(P->pi, nb, wt, (const cplx<R>*)P->xbuf.p,
                                                               (const cplx<R>*)P->ebuf.p, eo, ho)));
     FM_CK(cudaGetLastError());
     if (!keep) {
-      FM_CK(cudaMemcpyAsync(E + (size_t)b0 * 3 * g * 2, eo, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
-      FM_CK(cudaMemcpyAsync(H + (size_t)b0 * 3 * g * 2, ho, (size_t)nb * 3 * g * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+      FM_CK(cudaEventRecord(P->ready[slot], P->st));
+      pend[slot] = std::async(std::launch::async, copy_out, P, slot, (const void*)eo, (const void*)ho,
+                              (void*)(E + (size_t)b0 * 3 * g * 2), (void*)(H + (size_t)b0 * 3 * g * 2),
+                              (size_t)nb * 3 * g * sizeof(double2));
     }
     FM_CK(cudaStreamSynchronize(P->st));
     tk_resolve(P);
@@ -2095,6 +2204,8 @@ static fm_status solve_waves_t(fm_plan* P, int nrhs, const int* first, const fm_
       all_ok &= inf[b].solved != 0;
     }
   }
+  for (auto& f : pend)
+    if (f.valid()) FM_CK(f.get());
   P->out_nrhs = keep ? nrhs : 0;
   if (!all_ok) return fail(FM_NOT_CONVERGED, "iteration limit reached before the tolerance was met");
   return FM_OK;
@@ -2189,6 +2300,10 @@ fm_status fm_plan_set_tuning(fm_plan* P, int knob, int value) {
       if (value < 0) return fail(FM_ERR_INVALID, "right-hand sides per wave must be >= 0");
       P->wave_rhs = value;
       return FM_OK;
+    case FM_TUNE_BLOCK_DOT:
+      if (value != 0 && value != 1) return fail(FM_ERR_INVALID, "block-dot tuning value must be 0 or 1");
+      P->bd_bulk = value != 0;
+      return FM_OK;
     default:
       return fail(FM_ERR_INVALID, "unknown tuning knob");
   }
@@ -2202,6 +2317,7 @@ fm_status fm_plan_get_tuning(fm_plan* P, int knob, int* value) {
     case FM_TUNE_TMA_CTAS_PER_SM: *value = P->dims.tma_ctas; return FM_OK;
     case FM_TUNE_ROW_THREADS: *value = P->dims.row_threads; return FM_OK;
     case FM_TUNE_WAVE_RHS: *value = P->wave_rhs; return FM_OK;
+    case FM_TUNE_BLOCK_DOT: *value = P->bd_bulk ? 1 : 0; return FM_OK;
     default: return fail(FM_ERR_INVALID, "unknown tuning knob");
   }
 }

@@ -41,7 +41,7 @@ def test_invalid_tuning_values_rejected():
     plan = solver.plan()
     lib = _lib.lib()
     for knob, value in ((_lib.FM_TUNE_Y_TMA, 2), (_lib.FM_TUNE_ROW_THREADS, 512), (_lib.FM_TUNE_TMA_CTAS_PER_SM, -1),
-                        (_lib.FM_TUNE_WAVE_RHS, -3), (99, 0)):
+                        (_lib.FM_TUNE_WAVE_RHS, -3), (_lib.FM_TUNE_BLOCK_DOT, 2), (99, 0)):
         assert lib.fm_plan_set_tuning(plan.handle, knob, value) == _lib.FM_ERR_INVALID
     v = ctypes.c_int(-1)
     assert lib.fm_plan_get_tuning(plan.handle, _lib.FM_TUNE_ROW_THREADS, ctypes.byref(v)) == _lib.FM_OK
@@ -71,3 +71,27 @@ def test_autotuned_solve_batch_matches_untuned(tmp_path, monkeypatch):
     for a, b in zip(outs[True], outs[False]):
         assert rel(a.E, b.E) < 1e-5
         assert rel(a.H, b.H) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32-math64"])
+def test_waves_and_host_output_copies(precision):
+    """Right-hand sides solved in waves of one (three waves, the two device output slots used in turn while the
+    copy of the previous wave to the host overlaps the next wave) equal the same batch in one wave."""
+    grid = (16, 16, 8)
+    ocfg, solver = configs(grid, absorbing_z(8), precision=precision,
+                           linear_solver=F.KrylovJL_GMRES(ortho="block", block_size=4))
+    med = F.Medium(bead(grid, 3.0), EPS_BG)
+    srcs = F.illumination_cone(grid, RES, WL, EPS_BG, 2, 1.2, 3)[:3]
+    outs = {}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for w in (0, 1):
+            AT.apply(solver.plan(), {"wave_rhs": w})
+            outs[w] = F.solve_batch(solver, [[s] for s in srcs], med)
+    AT.apply(solver.plan(), {"wave_rhs": 0})
+    tol = 1e-12 if precision == "float64" else 1e-6
+    for a, b in zip(outs[1], outs[0]):
+        assert np.all(np.isfinite(a.E)) and np.all(np.isfinite(a.H))
+        assert rel(a.E, b.E) < tol
+        assert rel(a.H, b.H) < tol
+    solver.release()

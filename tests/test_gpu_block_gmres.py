@@ -89,3 +89,35 @@ def test_block_gmres_rejects_restart_and_bad_sizes():
         ocfg, solver = configs(grid, absorbing_z(8), linear_solver=ls)
         with pytest.raises((ValueError, F._lib.FMError)):
             F.solve(solver, xpol()[1], F.Medium(bead(grid, 2.0), EPS_BG))
+
+
+@pytest.mark.parametrize("precision,block", [("float64", 4), ("float64", 7), ("float32-math64", 4),
+                                             ("float32", 3)])
+def test_bulk_block_dot_matches_register_block_dot(precision, block):
+    """The bulk-copy pipelined block dot (one CTA per SM over all active right-hand sides) against the
+    register-staged one, on a batch whose right-hand sides stop at different iterations, so the list of
+    active right-hand sides changes during the solve."""
+    from fmcuda import autotune as AT
+    grid = (16, 16, 8)
+    ls = F.KrylovJL_GMRES(ortho="block", block_size=block)
+    ocfg, solver = configs(grid, absorbing_z(8), tol=1e-4, precision=precision, linear_solver=ls)
+    med = F.Medium(bead(grid, 3.0), EPS_BG)
+    srcs = [F.PlaneWaveSource(wavelength=WL, polarization=[1, 0, 0], k_vector=[0, 0, 1]),
+            F.PlaneWaveSource(wavelength=WL, polarization=[0, 1, 0], k_vector=[0.6, 0, 0.8]),
+            F.PlaneWaveSource(wavelength=WL, polarization=[1, 0, 0], k_vector=[0, 0.8, 0.6])]
+    res = {}
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        for bulk in (1, 0):
+            AT.apply(solver.plan(), {"block_dot": bulk})
+            outs = F.solve_batch(solver, srcs, med)
+            res[bulk] = (outs, [i["iterations"] for i in solver.last_info])
+    AT.apply(solver.plan(), {"block_dot": AT.DEFAULT["block_dot"]})
+    tol = 1e-10 if precision == "float64" else 1e-5
+    assert len(set(res[1][1])) > 1, "right-hand sides should stop at different iterations"
+    if precision == "float64":
+        assert res[1][1] == res[0][1]
+    for a, b in zip(res[1][0], res[0][0]):
+        assert rel(a.E, b.E) < tol
+        assert rel(a.H, b.H) < tol
+    solver.release()
