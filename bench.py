@@ -507,8 +507,8 @@ def main():
     ap.add_argument("--impl", default="fmcuda", choices=["fmcuda", "reference"])
     ap.add_argument("--nrhs", type=int, default=64)
     ap.add_argument("--ortho", default="block", choices=["mgs", "cgs", "cgs2", "block"])
-    ap.add_argument("--block", type=int, default=4, help="vectors per block for --ortho block")
-    ap.add_argument("--block-store", default="fp64", choices=["fp64", "storage"],
+    ap.add_argument("--block", type=int, default=8, help="vectors per block for --ortho block")
+    ap.add_argument("--block-store", default="fp64-ortho", choices=["fp64", "storage", "fp64-ortho"],
                     help="raw block vectors in complex FP64 or in the plan's storage type")
     ap.add_argument("--accuracy-rhs", type=int, default=8, help="right-hand sides checked against plain FP64")
     ap.add_argument("--autotune", type=int, default=1, help="1: pick launch shapes and block size with fmcuda.autotune")

@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(BD_THREADS, 1)
           for (int q = 0; q < 4; ++q)
 #pragma unroll
             for (int jg = 0; jg < NG; ++jg) {
-              const double2 x = to_d_int(xv[jg][h][q]);
+              const double2 x = to_d(xv[jg][h][q]);
 #pragma unroll
               for (int t = 0; t < NT; ++t) {
                 mma_f64(P[jg][t][0], P[jg][t][1], x.x, bf[t][h][q]);

@@ -972,45 +972,63 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
   return cudaGetLastError();
 }
 
-template <typename R, typename YR, int S>
+// Z = Y - X E and the Gram matrix of Z.  TZ: type of Z (the basis type, or the block-vector type when the block
+// is stored orthonormalised afterwards and Z overwrites Y in place).
+template <typename R, typename YR, int S, typename TZ>
 static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, const void* Y, void* Z, const int* act,
                                       int nact) {
   using T = cplx<R>;
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S, TZ>, KV_THREADS, 0) !=
+          cudaSuccess ||
       bps < 1)
     bps = 1;
   const long long maxb = (P->M + 32 * KV_WARPS - 1) / (32 * KV_WARPS);
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
-  FM_TRACK(P, KC_UPD, ((double)(K + S) * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M,
-           (k_blockupdate_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, K, (const T*)U, (const TY*)Y, (T*)Z, (const double2*)P->coef.p, act)));
+  FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
+           (k_blockupdate_mma<R, TY, S, TZ><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z, (const double2*)P->coef.p, act)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int nblk_g = kv_blocks(P, k_blockgram<R, S>, nb);
+  const int nblk_g = kv_blocks(P, k_blockgram<R, S, TZ>, nb);
   e = P->red_part.ensure((size_t)nb * nblk_g * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
   if (e != cudaSuccess) return e;
-  FM_TRACK(P, KC_MGS, (double)S * sizeof(T) * nact * P->M,
-           (k_blockgram<R, S><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, (const T*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
+  FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
+           (k_blockgram<R, S, TZ><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, (const TZ*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
   return cudaGetLastError();
 }
 
+// V (basis slots) = Z Rb^{-1} for the orthonormalised block storage; coefficients in P->coef
+template <typename R, typename YR, int S>
+static cudaError_t launch_blocknorm(fm_plan* P, int nb, const void* Z, void* V, const int* act, int nact) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+  FM_TRACK(P, KC_AXPBY, (double)S * (sizeof(TY) + sizeof(T)) * nact * P->M,
+           (k_blocknorm<R, TY, S><<<dim3(kv_blocks(P, k_blocknorm<R, TY, S>, nb), nb), KV_THREADS, 0, P->st>>>(
+               P->M, nb, (const TY*)Z, (const double2*)P->coef.p, (T*)V, act)));
+  return cudaGetLastError();
+}
+
+// which: 0 block dot, 1 block update into the basis, 2 block update in place into Y, 3 orthonormalisation
 template <typename R, typename YR>
-static cudaError_t block_kernels(fm_plan* P, bool dot, int S, int nb, int K, const void* U, const void* Y, void* Z,
+static cudaError_t block_kernels(fm_plan* P, int which, int S, int nb, int K, const void* U, const void* Y, void* Z,
                                  const int* act, int nact) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+#define FM_BLK(SS)                                                                                     \
+  case SS:                                                                                             \
+    return which == 0   ? launch_blockdot<R, YR, SS>(P, nb, K, U, Y, act, nact)                        \
+           : which == 1 ? launch_blockupdate<R, YR, SS, T>(P, nb, K, U, Y, Z, act, nact)              \
+           : which == 2 ? launch_blockupdate<R, YR, SS, TY>(P, nb, K, U, Y, Z, act, nact)             \
+                        : launch_blocknorm<R, YR, SS>(P, nb, Y, Z, act, nact);
   switch (S) {
-    case 2: return dot ? launch_blockdot<R, YR, 2>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 2>(P, nb, K, U, Y, Z, act, nact);
-    case 3: return dot ? launch_blockdot<R, YR, 3>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 3>(P, nb, K, U, Y, Z, act, nact);
-    case 4: return dot ? launch_blockdot<R, YR, 4>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 4>(P, nb, K, U, Y, Z, act, nact);
-    case 5: return dot ? launch_blockdot<R, YR, 5>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 5>(P, nb, K, U, Y, Z, act, nact);
-    case 6: return dot ? launch_blockdot<R, YR, 6>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 6>(P, nb, K, U, Y, Z, act, nact);
-    case 7: return dot ? launch_blockdot<R, YR, 7>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 7>(P, nb, K, U, Y, Z, act, nact);
-    case 8: return dot ? launch_blockdot<R, YR, 8>(P, nb, K, U, Y, act, nact) : launch_blockupdate<R, YR, 8>(P, nb, K, U, Y, Z, act, nact);
+    FM_BLK(2) FM_BLK(3) FM_BLK(4) FM_BLK(5) FM_BLK(6) FM_BLK(7) FM_BLK(8)
     default: return cudaErrorInvalidValue;
   }
+#undef FM_BLK
 }
 
 // Block vectors are generated and kept in FP64 (YR = double) on FP64 and FP32-storage/FP64-arithmetic plans
@@ -1023,6 +1041,7 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
   using T = cplx<R>;
   using TY = cplx<YR>;
   const int S = block_size_of(o);
+  const bool ortho_store = o.block_store == FM_BLOCK_FP64_ORTHO;
   const size_t fe = (size_t)P->M;
   const size_t fbytes = (size_t)nb * fe * sizeof(T);
   const int itmax = std::max(1, o.maxiters);
@@ -1223,7 +1242,7 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       FM_TRY(green_op<YR>(P, nb, Yin, PRO_V, nullptr, EPI_PREC_OP, Yin, nullptr, eps, Yout, act, nact, &rcY));
     }
     // D = X^H Y_{1..S}
-    FM_CK((block_kernels<R, YR>(P, true, S, nb, K, U, Yb + (size_t)nb * fe, nullptr, act, nact)));
+    FM_CK((block_kernels<R, YR>(P, 0, S, nb, K, U, Yb + (size_t)nb * fe, nullptr, act, nact)));
     std::vector<double2> D((size_t)nb * K * S);
     FM_CK(cudaMemcpyAsync(D.data(), P->red_out.p, D.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     FM_CK(cudaStreamSynchronize(P->st));
@@ -1249,13 +1268,17 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       }
     }
     FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
-    // Y' = Y - X E into basis slots m+1..m+S, Gram of Y'
-    FM_CK((block_kernels<R, YR>(P, false, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
+    // Y' = Y - X E into basis slots m+1..m+S (orthonormalised storage: over Y in place), Gram of Y'
+    if (ortho_store)
+      FM_CK((block_kernels<R, YR>(P, 2, S, nb, K, U, Yb + (size_t)nb * fe, Yb + (size_t)nb * fe, act, nact)));
+    else
+      FM_CK((block_kernels<R, YR>(P, 1, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
     const int NG = S * (S + 1) / 2;
     std::vector<double2> Gt((size_t)nb * NG);
     FM_CK(cudaMemcpyAsync(Gt.data(), P->red_out.p, Gt.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     FM_CK(cudaStreamSynchronize(P->st));
     tk_resolve(P);
+    std::vector<double2> rbi(ortho_store ? (size_t)nb * S * S : 0, make_double2(0, 0));
     for (int b = 0; b < nb; ++b) {
       if (!acth[b]) continue;
       BlkState& r = St[b];
@@ -1272,9 +1295,27 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
         acth[b] = 0;
         continue;
       }
-      for (int u = 0; u < S; ++u) {
-        for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = Rb[a + (size_t)u * S];
-        r.b0[K + u] = K;
+      if (ortho_store) {
+        // stored columns V = Y' Rb^{-1} are orthonormal: identity diagonal blocks of Rf
+        for (int t = 0; t < S; ++t) {
+          std::vector<cd> col(S, 0.0);
+          col[t] = 1.0;
+          for (int i = t; i >= 0; --i) {
+            cd v = col[i];
+            for (int q = i + 1; q <= t; ++q) v -= Rb[i + (size_t)q * S] * col[q];
+            col[i] = v / Rb[i + (size_t)i * S];
+          }
+          for (int u = 0; u <= t; ++u) rbi[(size_t)b * S * S + u * S + t] = make_double2(col[u].real(), col[u].imag());
+        }
+        for (int u = 0; u < S; ++u) {
+          for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = (a == u) ? cd(1.0, 0.0) : cd(0.0, 0.0);
+          r.b0[K + u] = K + u;
+        }
+      } else {
+        for (int u = 0; u < S; ++u) {
+          for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = Rb[a + (size_t)u * S];
+          r.b0[K + u] = K;
+        }
       }
       r.nvec = K + S;
       // W: V coordinates of Y_0..Y_S, n x (S+1)
@@ -1311,6 +1352,10 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
           break;
         }
       }
+    }
+    if (ortho_store) {  // zero coefficients for right-hand sides whose block broke down: their slots stay unused
+      FM_CK(cudaMemcpyAsync(P->coef.p, rbi.data(), rbi.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+      FM_CK((block_kernels<R, YR>(P, 3, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
     }
     m += S;
     if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
@@ -1569,7 +1614,7 @@ static fm_status solve_core(fm_plan* P, int nb, const fm_solve_opts& o, std::vec
   FM_CK(cudaMemcpyAsync(P->xbuf.p, P->bbuf.p, fbytes, cudaMemcpyDeviceToDevice, P->st));
   fm_status st;
   if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK)
-    st = (P->c64 && o.block_store == FM_BLOCK_FP64) ? gmres_block<R, double>(P, nb, o, info, deadline)
+    st = (P->c64 && o.block_store != FM_BLOCK_STORAGE) ? gmres_block<R, double>(P, nb, o, info, deadline)
                                                     : gmres_block<R, R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_GMRES) st = gmres<R>(P, nb, o, info, deadline);
   else if (o.method == FM_METHOD_BICGSTAB) st = bicgstab<R>(P, nb, o, info, deadline);
@@ -1619,7 +1664,7 @@ static fm_status validate_opts(const fm_solve_opts* o) {
   if (o->ortho < 0 || o->ortho > 3) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
   if (o->ortho == FM_ORTHO_BLOCK && o->method == FM_METHOD_GMRES) {
     if (o->block != 0 && (o->block < 2 || o->block > 8)) return fail(FM_ERR_INVALID, "block size must be 2..8");
-    if (o->block_store != FM_BLOCK_FP64 && o->block_store != FM_BLOCK_STORAGE)
+    if (o->block_store != FM_BLOCK_FP64 && o->block_store != FM_BLOCK_STORAGE && o->block_store != FM_BLOCK_FP64_ORTHO)
       return fail(FM_ERR_INVALID, "unknown block vector storage");
     if (o->restart > 0) return fail(FM_ERR_UNSUPPORTED, "block GMRES runs full GMRES only (restart = 0)");
     if (o->maxiters + block_size_of(*o) + 1 > KV_KMAX)
@@ -1643,7 +1688,7 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   size_t extra = 0;  // block GMRES: FP64 block vectors, FP64 pass temporaries, FP64 potential
   if (o.method == FM_METHOD_GMRES && o.ortho == FM_ORTHO_BLOCK) {
     vecs = o.maxiters + block_size_of(o) + 1;
-    extra = (o.block_store == FM_BLOCK_FP64 && P->c64) ? (size_t)P->M * sizeof(double2) * (block_size_of(o) + 1 + 2)
+    extra = (o.block_store != FM_BLOCK_STORAGE && P->c64) ? (size_t)P->M * sizeof(double2) * (block_size_of(o) + 1 + 2)
                                                         : fb * (size_t)(block_size_of(o) + 1);
   }
   else if (o.method == FM_METHOD_BICGSTAB) vecs = 6;

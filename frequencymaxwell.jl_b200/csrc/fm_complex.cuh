@@ -40,20 +40,6 @@ template <typename T> __host__ __device__ __forceinline__ T czero() { return mk(
 
 __device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
 __device__ __forceinline__ double2 to_d(double2 a) { return a; }
-// FP32 -> FP64 by moving the IEEE-754 fields with integer instructions, which keeps the conversion unit free
-// for kernels that convert every element they stream: exact for normal numbers, zeros, infinities and NaNs;
-// FP32 subnormals (|x| < 2^-126) become a zero of the same sign.
-__device__ __forceinline__ double f2d_int(float f) {
-  const unsigned u = __float_as_uint(f);
-  const unsigned a = u & 0x7fffffffu;
-  unsigned hi = (a >> 3) + 0x38000000u;  // exponent bias 127 -> 1023: + (1023 - 127) << 20
-  unsigned lo = u << 29;
-  if (a >= 0x7f800000u) hi = 0x7ff00000u | (a >> 3);  // infinity / NaN
-  if (a < 0x00800000u) hi = lo = 0u;                   // zero / subnormal
-  return __hiloint2double((int)(hi | (u & 0x80000000u)), (int)lo);
-}
-__device__ __forceinline__ double2 to_d_int(float2 a) { return make_double2(f2d_int(a.x), f2d_int(a.y)); }
-__device__ __forceinline__ double2 to_d_int(double2 a) { return a; }
 template <typename T> __device__ __forceinline__ T from_d(double2 a);
 template <> __device__ __forceinline__ float2 from_d<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 template <> __device__ __forceinline__ double2 from_d<double2>(double2 a) { return a; }

@@ -465,9 +465,9 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
 // (lane gid: elements 4 gid .. 4 gid + 3 of the tile) and runs over the basis 4 vectors at a time.  B tiles
 // as in k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or  Re = P0[t] - Q1[t],
 // Im = P1[t] + Q0[t]  (two tiles).
-template <typename R, typename TY, int S>
+template <typename R, typename TY, int S, typename TZ = cplx<R>>
 __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
-                                                                const TY* Y, cplx<R>* Z,
+                                                                const TY* Y, TZ* Z,
                                                                 const double2* __restrict__ coef,
                                                                 const int* __restrict__ active) {
   static_assert(S >= 1 && S <= 8, "block update on tensor cores takes 1..8 block vectors");
@@ -493,7 +493,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
   const size_t us = (size_t)B * M;
   const T* ub = U + (size_t)b * M;
   const TY* yb = Y + (size_t)b * M;
-  T* zb = Z + (size_t)b * M;
+  TZ* zb = Z + (size_t)b * M;
   const long long tiles = (M + 31) / 32;
   for (long long tl = (long long)blockIdx.x * KV_WARPS + w; tl < tiles; tl += (long long)gridDim.x * KV_WARPS) {
     const long long ea = tl * 32 + 4 * gid;  // A rows of this lane: elements ea .. ea + 3 (wholly in or out)
@@ -536,11 +536,11 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
           const int t0 = 2 * tig;
           if (t0 < S) {
             const double2 y = to_d(yb[t0 * us + e]);
-            zb[t0 * us + e] = from_d<T>(make_double2(y.x - (P[q][0][0] - qp0), y.y - (pp0 + Q[q][0][0])));
+            zb[t0 * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][0] - qp0), y.y - (pp0 + Q[q][0][0])));
           }
           if (t0 + 1 < S) {
             const double2 y = to_d(yb[(t0 + 1) * us + e]);
-            zb[(t0 + 1) * us + e] = from_d<T>(make_double2(y.x - (P[q][0][1] - qp1), y.y - (pp1 + Q[q][0][1])));
+            zb[(t0 + 1) * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][1] - qp1), y.y - (pp1 + Q[q][0][1])));
           }
         }
       } else if (ein) {
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
           const int t = 2 * tig + i;
           if (t < S) {
             const double2 y = to_d(yb[t * us + e]);
-            zb[t * us + e] = from_d<T>(make_double2(y.x - (P[q][0][i] - Q[q][NT - 1][i]),
+            zb[t * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][i] - Q[q][NT - 1][i]),
                                                     y.y - (P[q][NT - 1][i] + Q[q][0][i])));
           }
         }
@@ -560,8 +560,8 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
 
 // Gram matrix of S stored vectors Z_t = Z[(t*B + b)*M]:  out[b][tri(t,u)] = <Z_t, Z_u>, t <= u,
 // tri(t,u) = t*S - t*(t-1)/2 + (u-t)   (FP64 accumulation, deterministic).
-template <typename R, int S>
-__global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, const cplx<R>* __restrict__ Z,
+template <typename R, int S, typename TZ = cplx<R>>
+__global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, const TZ* __restrict__ Z,
                                                           double2* __restrict__ part, double2* __restrict__ out,
                                                           unsigned* __restrict__ counter,
                                                           const int* __restrict__ active) {
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, co
   double2 gram[NG];
 #pragma unroll
   for (int i = 0; i < NG; ++i) gram[i] = make_double2(0.0, 0.0);
-  const cplx<R>* zb = Z + (size_t)b * M;
+  const TZ* zb = Z + (size_t)b * M;
   const size_t us = (size_t)B * M;
   const long long per = (M + nblk - 1) / nblk;
   const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
@@ -605,6 +605,46 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, co
     part[((size_t)b * nblk + blockIdx.x) * NG + i] = sum;
   }
   finish_reduce(part, out, counter, NG, nblk, b);
+}
+
+// Orthonormal block from the projected block vectors:  V_t[b] = sum_{u <= t} Z_u[b] c[b][u*S + t]
+// (c = Rb^{-1}, upper triangular), Z in the block-vector type, V in the basis type.
+template <typename R, typename TZ, int S>
+__global__ void __launch_bounds__(KV_THREADS, 2) k_blocknorm(long long M, int B, const TZ* __restrict__ Z,
+                                                          const double2* __restrict__ c, cplx<R>* __restrict__ V,
+                                                          const int* __restrict__ active) {
+  const int b = blockIdx.y;
+  if (active && !active[b]) return;
+  // coefficients are re-read from shared memory in the loop (volatile): held in registers they would take
+  // S*S complex values per thread and halve the resident warps
+  __shared__ double ccs[2 * S * S];
+  volatile double* cc = ccs;
+  if (threadIdx.x < S * S) {
+    const double2 v = c[(size_t)b * S * S + threadIdx.x];
+    ccs[2 * threadIdx.x] = v.x;
+    ccs[2 * threadIdx.x + 1] = v.y;
+  }
+  __syncthreads();
+  const size_t us = (size_t)B * M;
+  const TZ* zb = Z + (size_t)b * M;
+  cplx<R>* vb = V + (size_t)b * M;
+#pragma unroll 1
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < M; e += (long long)gridDim.x * blockDim.x) {
+    double2 z[S];
+#pragma unroll
+    for (int u = 0; u < S; ++u) z[u] = to_d(zb[u * us + e]);
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u <= t; ++u) {
+        const double2 w = make_double2(cc[2 * (u * S + t)], cc[2 * (u * S + t) + 1]);
+        acc.x = fma(w.x, z[u].x, fma(-w.y, z[u].y, acc.x));
+        acc.y = fma(w.x, z[u].y, fma(w.y, z[u].x, acc.y));
+      }
+      vb[t * us + e] = from_d<cplx<R>>(acc);
+    }
+  }
 }
 
 // Generic batched elementwise combination (FP64 arithmetic):

@@ -50,11 +50,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
+// try_wait with a suspend-time hint: the waiting thread is parked by the hardware until the phase completes
+// or about `ns` nanoseconds pass, instead of spinning on issue slots the working warps need
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t* bar, uint32_t parity, uint32_t ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+constexpr uint32_t TMA_SUSPEND_NS = 1000000u;  // 1 ms per parked try_wait
+
 // Bounded wait; returns false (and records `code` in *err) on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
   if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
-  while (!mbar_try_wait(bar, parity)) {
+  while (!mbar_try_wait_for(bar, parity, TMA_SUSPEND_NS)) {
     if (gtimer() - t0 > TMA_WAIT_NS) {
       if (err) atomicExch(err, code);
       return false;

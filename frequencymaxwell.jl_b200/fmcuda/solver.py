@@ -33,12 +33,13 @@ class KrylovJL_GMRES:
     """GMRES as LinearSolve's KrylovJL_GMRES runs it (default: no restart).  ``gmres_restart`` > 0
     gives GMRES(m).  ``ortho`` picks the Gram-Schmidt variant ("mgs" as Krylov.jl, "cgs", "cgs2", or "block":
     s-step GMRES with ``block_size`` vectors per block, full GMRES only; ``block_vectors`` "fp64" keeps the raw
-    block vectors in complex FP64 on plans that compute in FP64, "storage" in the plan's storage type);
+    block vectors in complex FP64 on plans that compute in FP64, "storage" in the plan's storage type,
+    "fp64-ortho" as "fp64" and stores each block orthonormalised);
     None chooses MGS for FP64 (Krylov.jl's choice) and classical Gram-Schmidt for the FP32 forms."""
     gmres_restart: int = 0
     ortho: Optional[str] = None
-    block_size: int = 4
-    block_vectors: str = "fp64"
+    block_size: int = 8
+    block_vectors: str = "fp64-ortho"
 
 
 @dataclass(frozen=True)
@@ -154,7 +155,8 @@ class ConvergentBornSolver:
             ortho = ls.ortho or ("mgs" if self.precision == "float64" else "cgs")
             o.ortho = _ORTHO[ortho]
             o.block = int(ls.block_size) if ortho == "block" else 0
-            o.block_store = {"fp64": L.FM_BLOCK_FP64, "storage": L.FM_BLOCK_STORAGE}[ls.block_vectors]
+            o.block_store = {"fp64": L.FM_BLOCK_FP64, "storage": L.FM_BLOCK_STORAGE,
+                             "fp64-ortho": L.FM_BLOCK_FP64_ORTHO}[ls.block_vectors]
             o.restart = int(ls.gmres_restart)
         elif isinstance(ls, KrylovJL_BICGSTAB):
             o.method = L.FM_METHOD_BICGSTAB

@@ -53,8 +53,11 @@ enum { FM_ORTHO_MGS = 0, FM_ORTHO_CGS = 1, FM_ORTHO_CGS2 = 2, FM_ORTHO_BLOCK = 3
 /* FM_ORTHO_BLOCK: type of the raw block vectors before they are orthogonalised.  FM_BLOCK_FP64 keeps them in
  * complex FP64 on plans that compute in FP64 (FM_PREC_F64, FM_PREC_F32_MATH64), which keeps the accuracy of
  * classical Gram-Schmidt; FM_BLOCK_STORAGE keeps them in the plan's storage type (less traffic, larger
- * rounding error on FP32-storage plans). */
-enum { FM_BLOCK_FP64 = 0, FM_BLOCK_STORAGE = 1 };
+ * rounding error on FP32-storage plans).  FM_BLOCK_FP64_ORTHO is FM_BLOCK_FP64 that also keeps the projected
+ * block in FP64 and stores it orthonormalised (V = Y' Rb^{-1}) instead of raw: the rounding of the stored basis
+ * is then not amplified by the condition number of the block, at the cost of one more pass over the S new
+ * vectors per block. */
+enum { FM_BLOCK_FP64 = 0, FM_BLOCK_STORAGE = 1, FM_BLOCK_FP64_ORTHO = 2 };
 
 typedef struct fm_plan fm_plan;
 
@@ -81,7 +84,7 @@ typedef struct {
   double abstol;        /* solver.tolerance * 1e-2 (convergent_born.jl:745) */
   double timeout_s;     /* host-side deadline for the whole call, 0 = none */
   int block;            /* FM_ORTHO_BLOCK: vectors per block, 2..8 (0: 4); ignored otherwise */
-  int block_store;      /* FM_ORTHO_BLOCK: FM_BLOCK_FP64 or FM_BLOCK_STORAGE; ignored otherwise */
+  int block_store;      /* FM_ORTHO_BLOCK: FM_BLOCK_FP64, FM_BLOCK_STORAGE or FM_BLOCK_FP64_ORTHO; ignored otherwise */
 } fm_solve_opts;
 
 typedef struct {

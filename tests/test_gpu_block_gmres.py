@@ -72,7 +72,7 @@ def test_block_gmres_batch_equals_single():
             assert rel(o.H, one.H) < 1e-12
 
 
-@pytest.mark.parametrize("store", ["fp64", "storage"])
+@pytest.mark.parametrize("store", ["fp64", "storage", "fp64-ortho"])
 def test_block_gmres_oblique_fp32_math64(store):
     """Both kinds of raw block vectors on the FP32-storage / FP64-arithmetic plan."""
     grid = (32, 32, 16)
@@ -121,3 +121,22 @@ def test_bulk_block_dot_matches_register_block_dot(precision, block):
         assert rel(a.E, b.E) < tol
         assert rel(a.H, b.H) < tol
     solver.release()
+
+
+@pytest.mark.parametrize("precision,block", [("float64", 4), ("float64", 8), ("float32-math64", 4),
+                                             ("float32-math64", 8)])
+def test_block_gmres_orthonormal_block_storage(precision, block):
+    """Blocks stored orthonormalised (V = Y' Rb^{-1}) take the iterates of full GMRES like raw storage."""
+    ref, out, solver = _solve((32, 32, 16), 4.0, precision, block, store="fp64-ortho")
+    if precision == "float64":
+        assert solver.iteration_count == ref.iterations
+        assert abs(solver.residual_history[-1] - ref.residual) <= 1e-8 * ref.residual
+    assert rel(out.E, ref.E) < SOLVE_TOL[precision]
+    assert rel(out.H, ref.H) < SOLVE_TOL[precision]
+
+
+def test_block_gmres_orthonormal_storage_stops_inside_a_block():
+    ref, out, solver = _solve((16, 16, 8), 2.0, "float64", 4, tol=1e-3, store="fp64-ortho")
+    assert ref.solved and ref.iterations < 30
+    assert solver.iteration_count == ref.iterations
+    assert rel(out.E, ref.E) < 1e-10
