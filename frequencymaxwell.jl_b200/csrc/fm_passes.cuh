@@ -294,7 +294,8 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
         const R k2 = kx * kx + ky * ky + kz * kz;
         const R dr = k2 - ksr, di = -ksi;
         const R dd = dr * dr + di * di;
-        const T f = cmul(sc, mk(dr / dd, -di / dd));
+        const R rdd = R(1) / dd;  // one division for both parts of 1 / (k^2 - ks)
+        const T f = cmul(sc, mk(dr * rdd, -di * rdd));
         v[0][e] = cmul(csub(e1, cscale(kE, kx)), f);
         v[1][e] = cmul(csub(e2, cscale(kE, ky)), f);
         v[2][e] = cmul(csub(e3, cscale(kE, kz)), f);
