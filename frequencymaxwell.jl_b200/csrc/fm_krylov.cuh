@@ -503,15 +503,24 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int n = 0; n < NT; ++n) P[q][n][0] = P[q][n][1] = Q[q][n][0] = Q[q][n][1] = 0.0;
+    // the next 4 basis vectors are loaded before this step's MMAs: two loads in flight per lane
+    T xn[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      xn[q].x = 0;
+      xn[q].y = 0;
+    }
+    if (tig < K && ein) load4(ub + (size_t)tig * us + ea, xn);
     for (int k0 = 0; k0 < K; k0 += 4) {
-      const int k = k0 + tig;
       T xv[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        xv[q].x = 0;
-        xv[q].y = 0;
+        xv[q] = xn[q];
+        xn[q].x = 0;
+        xn[q].y = 0;
       }
-      if (k < K && ein) load4(ub + (size_t)k * us + ea, xv);
+      const int kn = k0 + 4 + tig;
+      if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xn);
       double bfr[NT];
 #pragma unroll
       for (int n = 0; n < NT; ++n) bfr[n] = Bs[k0 + tig][8 * n + gid];  // rows past K are zero
