@@ -1726,8 +1726,10 @@ long long fm_plan_bytes(const fm_plan_desc* d, int nrhs, int basis) {
   long long n = 1;
   for (int a = 0; a < 3; ++a) n *= (long long)(d->grid[a] + 2 * d->pad[a]);
   const long long fb = 3 * n * (d->precision == FM_PREC_F64 ? 16 : 8);
+  // basis + six work fields per right-hand side, the potential, and the FP64 E/H outputs in two slots (host
+  // outputs are copied from one slot while the next wave fills the other)
   return fb * (long long)nrhs * (basis + 6) + n * (d->precision == FM_PREC_F64 ? 16 : 8) +
-         3LL * n * 16 * nrhs;
+         4LL * 3 * n * 16 * nrhs;
 }
 
 fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
