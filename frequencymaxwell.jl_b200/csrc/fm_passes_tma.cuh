@@ -35,7 +35,7 @@ struct YTmaCfg {
   static constexpr int CW = (TX / PW) < 4 ? (TX / PW) : 4;
   static constexpr int ROUNDS = TX / (CW * PW);
   static constexpr int TILE = L * 128;
-  static constexpr int NST = TILE <= 16384 ? 4 : (TILE <= 32768 ? 3 : 2);
+  static constexpr int NST = TILE <= 32768 ? 3 : 2;  // three stages leave room for three CTAs per SM
   static constexpr int STRIDE = PencilStride<L, T, P::TP, true>::v;
   using SM = TmaSmem<TILE, NST, CW * PW * STRIDE * (int)sizeof(T), L * (int)sizeof(T)>;
   static constexpr int THREADS = CW * 32;
