@@ -339,7 +339,7 @@ struct EpiParams {
 };
 
 template <typename S, typename R, int L, int EPI>
-__global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
+__global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 3 : 1) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
                                             const cplx<S>* __restrict__ xv, const cplx<S>* __restrict__ bv,
                                             const double* __restrict__ rhs_scale, EpiParams ep,
                                             const cplx<R>* __restrict__ twx, const cplx<R>* __restrict__ rampx,
@@ -362,15 +362,11 @@ __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xi(Dims 
   if (active && !active[b]) return;
   const long long yz = row - (long long)b * d.ny * d.nz;
   T* sm = warp_smem<T, PencilStride<L, T, TP, true>::v>(ex, wic, PW, p);
-  T gam[E];
-  if constexpr (EPI == EPI_PREC_OP || EPI == EPI_PREC_RES) {
-    const R ie = ep.inv_eps_b ? (R)ep.inv_eps_b[b] : (R)ep.inv_eps;
-#pragma unroll
-    for (int e = 0; e < E; ++e) {
-      T vv = cv<T>(V[b * d.vstride + yz * L + lay_idx<L, E, P_::R0>(t, e)]);
-      gam[e] = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
-    }
-  }
+  // (i/eps) V is formed per component from V (an L1 hit after the first component) rather than held across
+  // the three components: the registers it would take decide how many CTAs fit on an SM
+  const R ie = (EPI == EPI_PREC_OP || EPI == EPI_PREC_RES) ? (ep.inv_eps_b ? (R)ep.inv_eps_b[b] : (R)ep.inv_eps) : R(0);
+  const cplx<S>* Vrow = V + b * d.vstride + yz * L;
+  const T shf = (EPI == EPI_PREC_OP && ep.shift_b) ? mk((R)ep.shift_b[b].x, (R)ep.shift_b[b].y) : czero<T>();
   R s = R(1);
   if (rhs_scale) s = (R)rhs_scale[b];
   const T al = mk((R)ep.alpha_re, (R)ep.alpha_im), be = mk((R)ep.beta_re, (R)ep.beta_im);
@@ -400,12 +396,16 @@ __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xi(Dims 
         if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(outb[ix])));
         r = a;
       } else if constexpr (EPI == EPI_PREC_OP) {
+        const T vv = cv<T>(Vrow[x]);
+        const T gam = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
         T xx = cscale(cv<T>(xvb[ix]), s);
-        r = cmul(gam[e], csub(xx, g));
-        if (ep.shift_b) r = csub(r, cmul(mk((R)ep.shift_b[b].x, (R)ep.shift_b[b].y), xx));
+        r = cmul(gam, csub(xx, g));
+        if (ep.shift_b) r = csub(r, cmul(shf, xx));
       } else {
+        const T vv = cv<T>(Vrow[x]);
+        const T gam = mk(-vv.y * ie, vv.x * ie);
         T xx = cscale(cv<T>(xvb[ix]), s);
-        r = cmul(gam[e], cadd(csub(cv<T>(bvb[ix]), xx), g));
+        r = cmul(gam, cadd(csub(cv<T>(bvb[ix]), xx), g));
       }
       outb[ix] = cv<TS>(r);
     }
