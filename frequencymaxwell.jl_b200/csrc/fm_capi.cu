@@ -2146,16 +2146,18 @@ static fm_status ensure_copier(fm_plan* P) {
 }
 
 static void host_copy(char* dst, const char* src, size_t n) {
-  constexpr int NT = 4;
+  // the first write to a fresh pageable destination faults its pages in: several threads take the faults in parallel
+  static const int NT = std::max(2, std::min(8, (int)std::thread::hardware_concurrency() / 2));
   if (n < ((size_t)4 << 20)) {
     std::memcpy(dst, src, n);
     return;
   }
   const size_t part = ((n + NT - 1) / NT + 63) & ~(size_t)63;
-  std::thread th[NT - 1];
+  std::vector<std::thread> th;
+  th.reserve(NT - 1);
   for (int i = 1; i < NT; ++i) {
     const size_t a = std::min(n, part * i), b = std::min(n, part * (i + 1));
-    th[i - 1] = std::thread([=] { std::memcpy(dst + a, src + a, b - a); });
+    if (b > a) th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
   }
   std::memcpy(dst, src, std::min(n, part));
   for (auto& t : th) t.join();

@@ -11,8 +11,8 @@ GMRES changes the order of the Gram-Schmidt arithmetic, and every candidate keep
 * ``block``              -- vectors per block of block GMRES (8 or 4)
 
 ``autotune`` times short fixed-work solves of the caller's own batch (tolerance 0, a few iterations) on the
-device, changes one knob at a time from the current best (coordinate search, two sweeps), and keeps the
-fastest.  Results are cached per device, grid, padding, precision, batch size and Gram-Schmidt variant, in
+device (best of 3), changes one knob at a time from the current best (coordinate search, two sweeps), and keeps
+a change only when it is more than 2 % faster.  Results are cached per device, grid, padding, precision, batch size and Gram-Schmidt variant, in
 memory and in a JSON file (``$FMCUDA_CACHE`` or ``~/.cache/fmcuda/autotune.json``).
 """
 from __future__ import annotations
@@ -95,6 +95,10 @@ def read(plan) -> dict:
     return out
 
 
+# a knob changes only for a gain above the trials' run-to-run spread (about 1 % for one-second trials)
+MIN_GAIN = 0.02
+
+
 def coordinate_search(measure: Callable[[dict], float], start: dict, space: Dict[str, Sequence],
                       sweeps: int = 2) -> (dict, Dict[str, float]):
     """Greedy search: from ``start``, try each alternative value of one knob at a time and keep any
@@ -118,7 +122,7 @@ def coordinate_search(measure: Callable[[dict], float], start: dict, space: Dict
                 cand = dict(best)
                 cand[knob] = v
                 t = timed(cand)
-                if t < t_best * 0.99:
+                if t < t_best * (1.0 - MIN_GAIN):
                     best, t_best, improved = cand, t, True
         if not improved:
             break
@@ -160,7 +164,7 @@ def autotune(solver, sources_list, medium, trial_iters: Optional[int] = None, us
         best = float("inf")
         with warnings.catch_warnings():
             warnings.simplefilter("ignore", RuntimeWarning)
-            for _ in range(2):
+            for _ in range(3):
                 plan.synchronize()
                 t0 = time.perf_counter()
                 plan.solve_plane_waves(lists, medium.permittivity_bg, opts, keep_on_device=True)
