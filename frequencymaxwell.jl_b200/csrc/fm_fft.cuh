@@ -192,46 +192,6 @@ __device__ __forceinline__ void fft_run(T (&v)[E], T* sm, const T* tw, int t) {
   }
 }
 
-// Three independent pencils (the three field components of one point column) through the same radix sequence,
-// each with its own exchange buffer, one step at a time: their instruction streams interleave between the warp
-// barriers, which gives the FP64 pipe three independent chains instead of one.
-template <int DIR, int L, int E, int R0, int R1, int R2, typename T>
-__device__ __forceinline__ void fft_run3(T (&v0)[E], T (&v1)[E], T (&v2)[E], T* s0, T* s1, T* s2, const T* tw,
-                                         int t) {
-  static_assert(R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) == L, "radices must multiply to L");
-  if constexpr (R1 == 0) {
-    fft_stage<DIR, L, E, R0, 1, true>(v0, s0, tw, t);
-    fft_stage<DIR, L, E, R0, 1, true>(v1, s1, tw, t);
-    fft_stage<DIR, L, E, R0, 1, true>(v2, s2, tw, t);
-  } else {
-    fft_stage<DIR, L, E, R0, 1, false>(v0, s0, tw, t);
-    fft_stage<DIR, L, E, R0, 1, false>(v1, s1, tw, t);
-    fft_stage<DIR, L, E, R0, 1, false>(v2, s2, tw, t);
-    __syncwarp();
-    fft_gather<L, E, R1>(v0, s0, t);
-    fft_gather<L, E, R1>(v1, s1, t);
-    fft_gather<L, E, R1>(v2, s2, t);
-    __syncwarp();
-    if constexpr (R2 == 0) {
-      fft_stage<DIR, L, E, R1, R0, true>(v0, s0, tw, t);
-      fft_stage<DIR, L, E, R1, R0, true>(v1, s1, tw, t);
-      fft_stage<DIR, L, E, R1, R0, true>(v2, s2, tw, t);
-    } else {
-      fft_stage<DIR, L, E, R1, R0, false>(v0, s0, tw, t);
-      fft_stage<DIR, L, E, R1, R0, false>(v1, s1, tw, t);
-      fft_stage<DIR, L, E, R1, R0, false>(v2, s2, tw, t);
-      __syncwarp();
-      fft_gather<L, E, R2>(v0, s0, t);
-      fft_gather<L, E, R2>(v1, s1, t);
-      fft_gather<L, E, R2>(v2, s2, t);
-      __syncwarp();
-      fft_stage<DIR, L, E, R2, R0 * R1, true>(v0, s0, tw, t);
-      fft_stage<DIR, L, E, R2, R0 * R1, true>(v1, s1, tw, t);
-      fft_stage<DIR, L, E, R2, R0 * R1, true>(v2, s2, tw, t);
-    }
-  }
-}
-
 // ---- per-length plans ----
 // E elements per lane and the forward radix sequence; TP = L/E lanes per pencil, 4 <= TP <= 32
 // (so at most 8 pencils share a warp and every axis of >= 8 points tiles a warp).
@@ -271,19 +231,6 @@ __device__ __forceinline__ void fft_rev_plan(T (&v)[P::E], T* sm, const T* tw_re
   if constexpr (P::R1 == 0) fft_run<DIR, P::L, P::E, P::R0, 0, 0>(v, sm, tw_rev, t);
   else if constexpr (P::R2 == 0) fft_run<DIR, P::L, P::E, P::R1, P::R0, 0>(v, sm, tw_rev, t);
   else fft_run<DIR, P::L, P::E, P::R2, P::R1, P::R0>(v, sm, tw_rev, t);
-}
-
-template <int DIR, typename P, typename T>
-__device__ __forceinline__ void fft_fwd_plan3(T (&v0)[P::E], T (&v1)[P::E], T (&v2)[P::E], T* s0, T* s1, T* s2,
-                                              const T* tw_fwd, int t) {
-  fft_run3<DIR, P::L, P::E, P::R0, P::R1, P::R2>(v0, v1, v2, s0, s1, s2, tw_fwd, t);
-}
-template <int DIR, typename P, typename T>
-__device__ __forceinline__ void fft_rev_plan3(T (&v0)[P::E], T (&v1)[P::E], T (&v2)[P::E], T* s0, T* s1, T* s2,
-                                              const T* tw_rev, int t) {
-  if constexpr (P::R1 == 0) fft_run3<DIR, P::L, P::E, P::R0, 0, 0>(v0, v1, v2, s0, s1, s2, tw_rev, t);
-  else if constexpr (P::R2 == 0) fft_run3<DIR, P::L, P::E, P::R1, P::R0, 0>(v0, v1, v2, s0, s1, s2, tw_rev, t);
-  else fft_run3<DIR, P::L, P::E, P::R2, P::R1, P::R0>(v0, v1, v2, s0, s1, s2, tw_rev, t);
 }
 
 // Padded pencil stride in the exchange buffer.  A shared-memory wavefront serves

@@ -176,8 +176,7 @@ struct ZTmaCfg {
   static constexpr int TILE = 3 * L * 128;
   static constexpr int NST = TILE <= 32768 ? 3 : 2;
   static constexpr int STRIDE = PencilStride<LF, T, P::TP, true>::v;
-  // one exchange buffer per field component, so the three transforms interleave (fft_run3)
-  using SM = TmaSmem<TILE, NST, 3 * CW * PW * STRIDE * (int)sizeof(T), (2 * LF + L) * (int)sizeof(T)>;
+  using SM = TmaSmem<TILE, NST, CW * PW * STRIDE * (int)sizeof(T), (2 * LF + L) * (int)sizeof(T)>;
   static constexpr int THREADS = CW * 32;
 };
 
@@ -228,9 +227,7 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
     }
   }
   const int p = lane / TP, t = lane % TP;
-  T* xs0 = ex + ((0 * CW + warp) * PW + p) * C::STRIDE;
-  T* xs1 = ex + ((1 * CW + warp) * PW + p) * C::STRIDE;
-  T* xs2 = ex + ((2 * CW + warp) * PW + p) * C::STRIDE;
+  T* sm = ex + (warp * PW + p) * C::STRIDE;
   const R ksr = (R)gp.ksq_re;
   const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
   int it = 0;
@@ -264,9 +261,9 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
           }
           v[c][e] = a;
         }
+        fft_fwd_plan<-1, P_>(v[c], sm, tw, t);
+        __syncwarp();
       }
-      fft_fwd_plan3<-1, P_>(v[0], v[1], v[2], xs0, xs1, xs2, tw, t);
-      __syncwarp();
       R kx, ky;
       if (MODE == ZMODE_CURL) {
         kx = (R)gp.dk[0] * kidx_curl<R>(x, d.nx);
@@ -305,10 +302,10 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
           v[2][e] = cmul(csub(e3, cscale(kE, kz)), f);
         }
       }
-      fft_rev_plan3<+1, P_>(v[0], v[1], v[2], xs0, xs1, xs2, twr, t);
-      __syncwarp();
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
+        fft_rev_plan<+1, P_>(v[c], sm, twr, t);
+        __syncwarp();
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           const int z = lay_idx<LF, E, P_::R0>(t, e);
