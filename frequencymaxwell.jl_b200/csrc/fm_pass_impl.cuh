@@ -11,7 +11,7 @@ static void allow_smem(K kern, size_t bytes) {
 }
 
 constexpr int ROW_THREADS = 256;  // default threads per block of the row passes
-constexpr int ZG_THREADS = 128;
+constexpr int ZG_THREADS = ZG_WARPS * 32;
 // threads per block of the x and y row passes: 128 or 256 (the tuning value in Dims), else the default
 static inline int row_threads(const Dims& d) { return d.row_threads == 128 ? 128 : ROW_THREADS; }
 
@@ -79,6 +79,16 @@ static cudaError_t zg_L(const Dims& d, const void* in, const GreenParams& gp, co
   const long long warps = (long long)(d.nx / PW) * d.ny * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
   const size_t smem = (size_t)(2 * LF + L + W * PW * PencilStride<LF, T, P_::TP, false>::v) * sizeof(T);
+  // one pencil per warp and FP32 storage: stage the CTA's column block for coalesced loads and stores
+  if constexpr (PW == 1 && std::is_same<S, float>::value) {
+    if (d.nx % W == 0) {
+      const size_t smem_s = smem + (size_t)3 * L * W * sizeof(TS);
+      allow_smem(k_zg<S, R, L, MODE, true>, smem_s);
+      k_zg<S, R, L, MODE, true><<<blocks, ZG_THREADS, smem_s, st>>>(d, (const TS*)in, gp, (const T*)tw, (const T*)rz,
+                                                                    (TS*)out, act);
+      return cudaGetLastError();
+    }
+  }
   allow_smem(k_zg<S, R, L, MODE>, smem);
   k_zg<S, R, L, MODE><<<blocks, ZG_THREADS, smem, st>>>(d, (const TS*)in, gp, (const T*)tw, (const T*)rz, (TS*)out,
                                                          act);

@@ -201,7 +201,13 @@ __device__ __forceinline__ R kidx_curl(int i, int n) {
   return (R)(i < (n >> 1) ? i : i - n);
 }
 
-template <typename S, typename R, int L, int MODE>
+constexpr int ZG_WARPS = 4;  // warps per CTA of the register z pass
+
+// STG (one pencil per warp only): the CTA's warps take x-consecutive pencils at the same (y, b), and the CTA stages
+// the 3 x L x W column block in shared memory with coalesced loads and stores (rows of W consecutive x values)
+// instead of each lane reading one value per z-plane.  The launcher uses it when nx is a multiple of the warps
+// per CTA, so every CTA's warps share (y, b) and leave together.
+template <typename S, typename R, int L, int MODE, bool STG = false>
 __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ in, GreenParams gp,
                                             const cplx<R>* __restrict__ twz, const cplx<R>* __restrict__ rz,
                                             cplx<S>* __restrict__ out, const int* __restrict__ active) {
@@ -210,6 +216,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
   constexpr int LF = (MODE == ZMODE_AVG2) ? 2 * L : L;
   using P_ = Plan<LF, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  static_assert(!STG || PW == 1, "the staged z pass takes one pencil per warp");
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tw = reinterpret_cast<T*>(smraw);
   T* twr = tw + LF;
@@ -232,6 +239,20 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
   const long long plane = (long long)d.nx * d.ny;
   const long long base0 = (long long)b * 3 * d.n + (long long)y * d.nx + x;
   T* sm = warp_smem<T, PencilStride<LF, T, TP, false>::v>(ex, wic, PW, p);
+  // staged block: row r = (c, z) holds the W pencils' values; the pencil slot is XOR-swizzled with bits 2.. of r,
+  // so 16 consecutive rows of one pencil fall in 16 distinct 8-byte bank slots
+  constexpr int W = STG ? ZG_WARPS : 1;
+  static_assert(!STG || W == 4, "the swizzle assumes 4 pencils per row");
+  auto tix = [](int r, int g) { return r * W + (g ^ ((r >> 2) & (W - 1))); };
+  TS* tile = reinterpret_cast<TS*>(ex + (size_t)(blockDim.x >> 5) * PW * PencilStride<LF, T, TP, false>::v);
+  const long long cbase = base0 - wic;  // the CTA's first pencil (x - wic)
+  if constexpr (STG) {
+    for (int i = threadIdx.x; i < 3 * L * W; i += blockDim.x) {
+      const int g = i % W, r = i / W, c = r / L, z = r - c * L;
+      tile[tix(r, g)] = in[cbase + (long long)c * d.n + (long long)z * plane + g];
+    }
+    __syncthreads();
+  }
 
   T v[3][E];
 #pragma unroll
@@ -241,7 +262,8 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
       const int z = lay_idx<LF, E, P_::R0>(t, e);
       T a = czero<T>();
       if (MODE != ZMODE_AVG2 || z < L) {
-        a = cv<T>(in[base0 + (long long)c * d.n + (long long)z * plane]);
+        if constexpr (STG) a = cv<T>(tile[tix(c * L + z, wic)]);
+        else a = cv<T>(in[base0 + (long long)c * d.n + (long long)z * plane]);
         if (MODE != ZMODE_CURL && rz) a = cmul(a, rtab[z]);
       }
       v[c][e] = a;
@@ -313,10 +335,27 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
       if (MODE != ZMODE_AVG2 || z < L) {
         T a = v[c][e];
         if (MODE != ZMODE_CURL && rz) a = cmul(a, cconj(rtab[z]));
-        const long long o = base0 + (long long)c * d.n + (long long)z * plane;
-        if (gp.accumulate) a = cadd(a, cv<T>(out[o]));
-        out[o] = cv<TS>(a);
+        if constexpr (STG) {
+          tile[tix(c * L + z, wic)] = cv<TS>(a);
+        } else {
+          const long long o = base0 + (long long)c * d.n + (long long)z * plane;
+          if (gp.accumulate) a = cadd(a, cv<T>(out[o]));
+          out[o] = cv<TS>(a);
+        }
       }
+    }
+  }
+  if constexpr (STG) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 3 * L * W; i += blockDim.x) {
+      const int g = i % W, r = i / W, c = r / L, z = r - c * L;
+      const long long o = cbase + (long long)c * d.n + (long long)z * plane + g;
+      TS a = tile[tix(r, g)];
+      if (gp.accumulate) {
+        const T s2 = cadd(cv<T>(a), cv<T>(out[o]));
+        a = cv<TS>(s2);
+      }
+      out[o] = a;
     }
   }
 }
