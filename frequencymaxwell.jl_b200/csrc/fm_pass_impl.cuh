@@ -62,6 +62,18 @@ static cudaError_t y_L(const Dims& d, const void* in, const void* tw, const void
   const int W = row_threads(d) / 32;
   const long long warps = (long long)(d.nx / PW) * d.nz * 3 * d.nb;
   const unsigned blocks = (unsigned)((warps + W - 1) / W);
+  // one pencil per warp and FP32 storage: four x-consecutive pencils per CTA, staged for coalesced rows
+  if constexpr (PW == 1 && std::is_same<S, float>::value) {
+    if (d.nx % YG_WARPS == 0) {
+      const unsigned blocks_s = (unsigned)((warps + YG_WARPS - 1) / YG_WARPS);
+      const size_t smem_s = (size_t)(L + YG_WARPS * PW * PencilStride<L, T, P_::TP, false>::v) * sizeof(T) +
+                            (size_t)L * YG_WARPS * sizeof(TS);
+      allow_smem(k_y<S, R, L, DIR, true>, smem_s);
+      k_y<S, R, L, DIR, true><<<blocks_s, YG_WARPS * 32, smem_s, st>>>(d, (const TS*)in, (const T*)tw,
+                                                                       (const T*)ramp, (TS*)out, act);
+      return cudaGetLastError();
+    }
+  }
   const size_t smem = (size_t)(L + W * PW * PencilStride<L, T, P_::TP, false>::v) * sizeof(T);
   allow_smem(k_y<S, R, L, DIR>, smem);
   k_y<S, R, L, DIR><<<blocks, W * 32, smem, st>>>(d, (const TS*)in, (const T*)tw, (const T*)ramp, (TS*)out, act);

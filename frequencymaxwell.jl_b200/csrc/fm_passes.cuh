@@ -116,7 +116,11 @@ __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 2 : 1) k_xf(Dims 
 // x columns at fixed (z, c, b); lane = t*P + p so consecutive lanes read
 // consecutive x.
 // ---------------------------------------------------------------------------
-template <typename S, typename R, int L, int DIR>
+// STG (one pencil per warp only): the CTA's warps (YG_WARPS) take x-consecutive pencils of one (z, c, b) plane
+// and the CTA stages the L x W block in shared memory with coalesced rows of W consecutive x values; the pencil
+// slot is XOR-swizzled with bits 2.. of the row.  The launcher uses it when nx is a multiple of the warps per CTA.
+constexpr int YG_WARPS = 4;
+template <typename S, typename R, int L, int DIR, bool STG = false>
 __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ in, const cplx<R>* __restrict__ twy,
                                            const cplx<R>* __restrict__ rampy, cplx<S>* __restrict__ out,
                                            const int* __restrict__ active) {
@@ -124,6 +128,7 @@ __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ i
   using TS = cplx<S>;
   using P_ = Plan<L, R>;
   constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  static_assert(!STG || PW == 1, "the staged y pass takes one pencil per warp");
   extern __shared__ __align__(16) unsigned char smraw[];
   T* tw = reinterpret_cast<T*>(smraw);
   T* ex = tw + L;
@@ -141,28 +146,55 @@ __global__ void __launch_bounds__(256) k_y(Dims d, const cplx<S>* __restrict__ i
   if (active && !active[b]) return;
   const long long base = zcb * (long long)d.ny * d.nx + x;
   T* sm = warp_smem<T, PencilStride<L, T, TP, false>::v>(ex, wic, PW, p);
+  constexpr int W = STG ? YG_WARPS : 1;
+  static_assert(!STG || W == 4, "the swizzle assumes 4 pencils per row");
+  auto tix = [](int r, int g) { return r * W + (g ^ ((r >> 2) & (W - 1))); };
+  TS* tile = reinterpret_cast<TS*>(ex + (size_t)(blockDim.x >> 5) * PW * PencilStride<L, T, TP, false>::v);
+  const long long cbase = base - wic;  // the CTA's first pencil
+  if constexpr (STG) {
+    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+      const int g = i % W, r = i / W;
+      tile[tix(r, g)] = in[cbase + (long long)r * d.nx + g];
+    }
+    __syncthreads();
+  }
+  auto ld = [&](int y) -> T {
+    if constexpr (STG) return cv<T>(tile[tix(y, wic)]);
+    else return cv<T>(in[base + (long long)y * d.nx]);
+  };
+  auto st = [&](int y, T a) {
+    if constexpr (STG) tile[tix(y, wic)] = cv<TS>(a);
+    else out[base + (long long)y * d.nx] = cv<TS>(a);
+  };
   T v[E];
   if constexpr (DIR < 0) {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int y = lay_idx<L, E, P_::R0>(t, e);
-      T a = cv<T>(in[base + (long long)y * d.nx]);
+      T a = ld(y);
       if (rampy) a = cmul(a, rampy[y]);
       v[e] = a;
     }
     fft_fwd_plan<-1, P_>(v, sm, tw, t);
 #pragma unroll
-    for (int e = 0; e < E; ++e) out[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx] = cv<TS>(v[e]);
+    for (int e = 0; e < E; ++e) st(lay_idx<L, E, P_::RL>(t, e), v[e]);
   } else {
 #pragma unroll
-    for (int e = 0; e < E; ++e) v[e] = cv<T>(in[base + (long long)lay_idx<L, E, P_::RL>(t, e) * d.nx]);
+    for (int e = 0; e < E; ++e) v[e] = ld(lay_idx<L, E, P_::RL>(t, e));
     fft_rev_plan<+1, P_>(v, sm, tw, t);
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int y = lay_idx<L, E, P_::R0>(t, e);
       T a = v[e];
       if (rampy) a = cmul(a, cconj(rampy[y]));
-      out[base + (long long)y * d.nx] = cv<TS>(a);
+      st(y, a);
+    }
+  }
+  if constexpr (STG) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < L * W; i += blockDim.x) {
+      const int g = i % W, r = i / W;
+      out[cbase + (long long)r * d.nx + g] = tile[tix(r, g)];
     }
   }
 }

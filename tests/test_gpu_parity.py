@@ -32,7 +32,7 @@ def _plan_with_oracle_potential(grid, bcs, precision):
 @pytest.mark.parametrize("grid,kind", [((32, 32, 16), "absz"), ((16, 32, 8), "absz"), ((32, 16, 32), "per"),
                                        ((64, 32, 32), "absz"), ((96, 32, 16), "absz"), ((32, 96, 16), "absz"),
                                        ((16, 32, 96), "per"), ((16, 16, 128), "absz"), ((16, 8, 512), "per"),
-                                       ((8, 16, 256), "absz")])
+                                       ((8, 16, 256), "absz"), ((8, 512, 8), "per")])
 def test_green_apply(precision, grid, kind):
     bcs = absorbing_z(grid[2]) if kind == "absz" else periodic()
     ocfg, solver, plan, pot = _plan_with_oracle_potential(grid, bcs, precision)
