@@ -20,6 +20,21 @@ const FM_NOT_CONVERGED = Cint(3)
 const FM_PREC_F64 = Cint(0)
 const FM_PREC_F32 = Cint(1)
 const FM_PREC_F32_MATH64 = Cint(2)
+const FM_METHOD_GMRES = Cint(0)
+const FM_METHOD_BICGSTAB = Cint(1)
+const FM_ORTHO_MGS = Cint(0)
+const FM_ORTHO_CGS = Cint(1)
+const FM_ORTHO_CGS2 = Cint(2)
+const FM_ORTHO_BLOCK = Cint(3)
+const FM_BLOCK_FP64 = Cint(0)
+const FM_BLOCK_STORAGE = Cint(1)
+const FM_BLOCK_FP64_ORTHO = Cint(2)
+const FM_TUNE_Y_TMA = Cint(0)
+const FM_TUNE_Z_TMA = Cint(1)
+const FM_TUNE_TMA_CTAS_PER_SM = Cint(2)
+const FM_TUNE_ROW_THREADS = Cint(3)
+const FM_TUNE_WAVE_RHS = Cint(4)
+const FM_TUNE_BLOCK_DOT = Cint(5)
 
 struct FMPlanDesc
     grid::NTuple{3,Cint}
@@ -72,12 +87,32 @@ function check(status)
     error("libfmcuda: " * msg)
 end
 
-function plan_desc(solver::ConvergentBornSolver{T}) where {T}
+function plan_desc(solver::ConvergentBornSolver{T}; max_rhs::Integer = 1) where {T}
     bcs = solver.boundary_conditions
     pad = ntuple(i -> FrequencyMaxwell.padding_pixels(bcs[i], solver.resolution[i]), 3)
     prec = T === Float64 ? FM_PREC_F64 : FM_PREC_F32_MATH64
     FMPlanDesc(Cint.(solver.grid_size), Cint.(pad), Cdouble.(solver.resolution),
-               ntuple(i -> Cint(FrequencyMaxwell.requires_averaging(bcs[i])), 3), prec, Cint(1), Cint(0))
+               ntuple(i -> Cint(FrequencyMaxwell.requires_averaging(bcs[i])), 3), prec, Cint(max_rhs), Cint(0))
+end
+
+plane_wave(s) = FMPlaneWave(s.wavelength,
+                            (real(s.polarization[1]), imag(s.polarization[1]), real(s.polarization[2]),
+                             imag(s.polarization[2]), real(s.polarization[3]), imag(s.polarization[3])),
+                            Tuple(Float64.(s.k_vector)), s.amplitude, s.phase)
+
+# device potential of `medium` on `plan`; returns Bornmax
+function build_potential!(plan, solver, medium, wavelength)
+    eps = ComplexF64.(FrequencyMaxwell.permittivity(medium))
+    fx, fy, fz = (attenuation_filter(solver, d) for d in 1:3)
+    pinfo = Ref{FMPotentialInfo}()
+    check(ccall((:fm_build_potential, libfmcuda), Cint,
+                (Ptr{Cvoid}, Ptr{ComplexF64}, Cdouble, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Cint,
+                 Ref{FMPotentialInfo}),
+                plan, eps, FrequencyMaxwell.permittivity_bg(medium), wavelength, fx, fy, fz,
+                solver.iterations_max, pinfo))
+    bornmax = Int(pinfo[].bornmax)
+    bornmax >= 1 || throw(ArgumentError("Bornmax < 1"))
+    return bornmax
 end
 
 # the per-axis filters of _apply_attenuation_to_potential! (convergent_born.jl:893-944)
@@ -139,6 +174,48 @@ function solve_fmcuda(solver::ConvergentBornSolver{T}, sources, medium) where {T
         solver.iteration_count = info[].iterations
         push!(solver.residual_history, T(info[].residual))
         return ElectromagneticField(Complex{T}.(E), Complex{T}.(H), solver.resolution, wavelength)
+    finally
+        ccall((:fm_plan_destroy, libfmcuda), Cvoid, (Ptr{Cvoid},), plan[])
+    end
+end
+
+"""
+    solve_fmcuda_batch(solver, sources_list, medium; block = 8) -> Vector{ElectromagneticField}
+
+Many illuminations of one medium (each element of `sources_list` a source or a vector of sources, coherently
+superposed) as the right-hand sides of one batched solve.  The batch uses s-step block GMRES with FP64 block
+vectors stored orthonormalised (`block` vectors per block), which takes the iterates of full GMRES.  It needs
+restart = 0 and at most 128 basis vectors: max(2 Bornmax, 100) + block + 1.
+"""
+function solve_fmcuda_batch(solver::ConvergentBornSolver{T}, sources_list, medium; block::Integer = 8) where {T}
+    FrequencyMaxwell.grid_size(medium) == solver.grid_size ||
+        throw(ArgumentError("medium grid_size must match solver grid_size"))
+    lists = [s isa AbstractVector ? s : [s] for s in sources_list]
+    isempty(lists) && throw(ArgumentError("sources_list cannot be empty"))
+    wavelength = FrequencyMaxwell.source_wavelength(lists[1])
+    n = length(lists)
+    desc = Ref(plan_desc(solver; max_rhs = n))
+    plan = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:fm_plan_create, libfmcuda), Cint, (Ref{FMPlanDesc}, Ref{Ptr{Cvoid}}), desc, plan))
+    try
+        bornmax = build_potential!(plan[], solver, medium, wavelength)
+        waves = [plane_wave(s) for l in lists for s in l]
+        first = Cint.(cumsum([0; length.(lists)]))
+        opts = Ref(FMSolveOpts(FM_METHOD_GMRES, FM_ORTHO_BLOCK, Cint(0), Cint(max(2bornmax, 100)),
+                               solver.tolerance, solver.tolerance * 1e-2, 0.0, Cint(block), FM_BLOCK_FP64_ORTHO))
+        E = Array{ComplexF64}(undef, solver.grid_size..., 3, n)
+        H = similar(E)
+        info = Vector{FMSolveInfo}(undef, n)
+        st = check(ccall((:fm_solve_plane_waves, libfmcuda), Cint,
+                         (Ptr{Cvoid}, Cint, Ptr{Cint}, Ptr{FMPlaneWave}, Cdouble, Ref{FMSolveOpts}, Ptr{ComplexF64},
+                          Ptr{ComplexF64}, Ptr{FMSolveInfo}),
+                         plan[], Cint(n), first, waves, FrequencyMaxwell.permittivity_bg(medium), opts, E, H, info))
+        st == FM_NOT_CONVERGED && @warn "LinearSolve.jl did not converge."
+        solver.Bornmax = bornmax
+        solver.iteration_count = info[end].iterations
+        push!(solver.residual_history, T(info[end].residual))
+        return [ElectromagneticField(Complex{T}.(E[:, :, :, :, b]), Complex{T}.(H[:, :, :, :, b]), solver.resolution,
+                                     wavelength) for b in 1:n]
     finally
         ccall((:fm_plan_destroy, libfmcuda), Cvoid, (Ptr{Cvoid},), plan[])
     end
