@@ -30,6 +30,31 @@ def test_library_exports_every_header_symbol():
     assert set(_lib.EXPORTED) == declared
 
 
+def _header_constants():
+    """FM_* enumerators and defines of include/fmcuda.h with their values."""
+    txt = open(os.path.join(ROOT, "include", "fmcuda.h")).read()
+    vals = {}
+    for body in re.findall(r"enum\s*\{([^}]*)\}", txt):
+        for name, v in re.findall(r"(FM_\w+)\s*=\s*(-?\d+)", body):
+            vals[name] = int(v)
+    return vals
+
+
+def test_binding_constants_match_the_header():
+    """The ctypes mirror and the Julia binding use the header's values for every constant they name."""
+    hdr = _header_constants()
+    assert {"FM_ORTHO_BLOCK", "FM_BLOCK_FP64_ORTHO", "FM_TUNE_BLOCK_DOT", "FM_PREC_F32_MATH64"} <= set(hdr)
+    py = {k: getattr(_lib, k) for k in dir(_lib) if k.startswith("FM_") and isinstance(getattr(_lib, k), int)}
+    for k, v in py.items():
+        if k in hdr:
+            assert hdr[k] == v, (k, v, hdr[k])
+    jl = open(os.path.join(ROOT, "frequencymaxwell.jl_b200", "julia", "FrequencyMaxwellCUDA.jl")).read()
+    named = dict((k, int(v)) for k, v in re.findall(r"const (FM_\w+) = Cint\((-?\d+)\)", jl))
+    assert len(named) >= 10
+    for k, v in named.items():
+        assert hdr.get(k) == v, (k, v, hdr.get(k))
+
+
 def test_library_loads_without_gpu_calls():
     L = _lib.lib()
     assert L.fm_abi_version() == 2
