@@ -1,8 +1,9 @@
 """Test helper: a numpy restatement of the library's s-step (block) GMRES with orthonormalised block storage.
 
 It follows the algebra of ``gmres_block`` in the CUDA library, written here with an explicit orthonormal basis:
-s classical Gram-Schmidt steps whose Ritz values (Leja-ordered) are the Newton shifts, then blocks of s operator
-applications Y_t = (M^-1 A - theta_t) Y_{t-1} from Y_0 = V_m, one block Gram-Schmidt projection, a Cholesky QR of
+s classical Gram-Schmidt steps whose Ritz values (Leja-ordered) are the first Newton shifts, then blocks of s operator
+applications Y_t = (M^-1 A - theta_t) Y_{t-1} from Y_0 = V_m (each block's shifts are the Ritz values of the
+previous block's diagonal Hessenberg block), one block Gram-Schmidt projection, a Cholesky QR of
 the projected block, and the Hessenberg columns recovered from (M^-1 A) V W_{0:s-1} = V (W_{1:s} + W_{0:s-1} theta).
 Givens rotations and the stopping test run column by column, as in ``oracle.cbs_oracle.gmres`` (Krylov.jl
 semantics), so in exact arithmetic the iterate is that of full GMRES.
@@ -129,6 +130,10 @@ def block_gmres(apply_A, apply_M, b, x0, atol, rtol, itmax, s):
                 state["done"] = True
                 break
         m += s
+        if not state["done"]:  # next shifts: Ritz values of this block's s x s diagonal Hessenberg block
+            Hs = np.array([[Hc[m - s + j][m - s + i] if m - s + i < len(Hc[m - s + j]) else 0 for j in range(s)]
+                           for i in range(s)])
+            theta = leja(list(np.linalg.eigvals(Hs)))
 
     k = len(R)
     y = list(z[:k])
