@@ -778,11 +778,13 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
 // device only sees raw combinations of stored vectors.
 //
 // After S classical Gram-Schmidt steps (which also give Ritz values for the
-// Newton shifts), each step from basis X_0..X_m (m = columns done):
-//   Y_0 = s0 X_m, Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}    (S operator applications)
+// first Newton shifts), each step from basis X_0..X_m (m = columns done):
+//   Y_0 = V_m, Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}       (S operator applications)
 //   D = X^H Y, C = Rf^{-H} D (projection in V coordinates)   (one sweep of the basis)
 //   Y' = Y - X Rf^{-1} C, G = Y'^H Y'                        (one sweep of the basis)
-//   G = Rb^H Rb (Cholesky); X_{m+1..m+S} = Y', Rf block = Rb
+//   G = Rb^H Rb (Cholesky); raw storage: X_{m+1..m+S} = Y', Rf block = Rb;
+//   orthonormalised storage: X_{m+1..m+S} = Y' Rb^{-1}, Rf block = I
+//   next shifts: Ritz values of this block's S x S diagonal Hessenberg block
 // and the Hessenberg columns m..m+S-1 follow from the relations
 //   (M^{-1}A) V W_{0:S-1} = V (W_{1:S} + W_{0:S-1} diag(theta)),
 // where W holds the V coordinates of Y_0..Y_S (block CA-GMRES change of
