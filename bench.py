@@ -2,18 +2,20 @@
 
 Workload (one "step"): the batching configuration -- 128x128x64 grid at 50 nm, water background
 (eps_bg = 1.33^2), a seeded phantom of 12 non-overlapping beads (radius U[4,12] px, index U[1.36,1.60]),
-64 right-hand sides (32 illumination angles in an NA 1.2 cone snapped to the lattice x 2 polarisations),
+64 right-hand sides per GPU (32 illumination angles in an NA 1.2 cone snapped to the lattice x 2 polarisations),
 500 nm, periodic x,y and absorbing z (padded grid 128^3), tolerance 1e-6, GMRES as the reference runs it
 (no restart, maxiters = max(2*Bornmax, 100), warm start b); complex64 fields in HBM, FFT / Green /
 potential arithmetic in FP64 registers, FP64 dots; the Krylov basis is built by block (s-step) GMRES with
-s = 4 (``--ortho cgs`` for classical Gram-Schmidt; ``--precision float32`` runs the arithmetic in FP32 too).
+s = 8 (``--ortho cgs`` for classical Gram-Schmidt; ``--precision float32`` runs the arithmetic in FP32 too).
+With N GPUs the job has 32N angles x 2 polarisations and each rank solves its own 64 (weak scaling).
 
 value : solves/s of that step with the potential resident in HBM and the fields left in HBM
-        (device time from CUDA events on the library's stream, max over ranks, weak scaling).
+        (device time from CUDA events on the library's stream, max over ranks).
 e2e   : solves/s through the public API (fmcuda.solve_batch) from host permittivity to host E, H.
-Also reported: the plain FP64 GPU method (same algorithm with Krylov.jl's MGS, one RHS) and the
-relative L2 distance of the batched FP32 fields to it, the roofline of the dominant kernel class from
-live CUDA-event timing, and the CPU oracle baseline (numpy/scipy FP64, all host cores, bounded sample).
+Also reported: the plain FP64 GPU method (same algorithm with Krylov.jl's MGS, one RHS), timed the same two ways,
+and the relative L2 distance of the batched FP32 fields to it; the CPU oracle's complete FP64 solve of RHS 0
+(the CPU baseline, and ``vs_oracle``: both GPU forms against it); the roofline of the dominant kernel class from
+live CUDA-event timing.
 
 `--impl reference` times the CPU restatement of the reference path (the reference is Julia, which this
 image does not have) on the same workload and prints its own line.
@@ -47,20 +49,21 @@ METRIC = "solves/s at rel-L2<=1e-5 vs FP64: batched FP32 vs plain FP64; p50/p99 
 
 
 def batching_sources(n_angles=32, seed=SEED):
-    """32 (kx, ky) uniform in the NA 1.2 disk (sin(theta) <= NA/n_bg), snapped to the lattice
-    2*pi*m/(N*dx); polarisations s and p (two unit vectors orthogonal to k)."""
+    """``n_angles`` (kx, ky) uniform in the NA 1.2 disk (sin(theta) <= NA/n_bg), snapped to the lattice
+    2*pi*m/(N*dx); polarisations s and p (two unit vectors orthogonal to k).  The first 32 angles do not depend
+    on ``n_angles``."""
     import fmcuda as F
     return [(s.k_vector, s.polarization.real) for s in
             F.illumination_cone(GRID, RES, WL, EPS_BG, n_angles, NA, seed)]
 
 
-def make_inputs():
+def make_inputs(n_angles=32):
     import fmcuda as F
     med = F.phantom_random_beads(GRID, 12, (4, 12), (1.36, 1.60), EPS_BG, SEED)
     bc_z = F.AbsorbingBoundaryCondition(thickness=GRID[2] * RES[2], attenuation_thickness=GRID[2] * RES[2],
                                         sharpness=1.0, profile=F.TanhProfile)
     bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
-    srcs = [F.PlaneWaveSource(wavelength=WL, polarization=p, k_vector=k) for k, p in batching_sources()]
+    srcs = [F.PlaneWaveSource(wavelength=WL, polarization=p, k_vector=k) for k, p in batching_sources(n_angles)]
     return med, bcs, srcs
 
 
@@ -123,61 +126,67 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(steps=1):
-    """Oracle (numpy/scipy FP64, all host cores) on a bounded sample of the workload: one RHS, the
-    set-up and right-hand side, two operator applications and 8 Gram-Schmidt projections are timed,
-    then the 100-iteration GMRES solve is assembled from the measured pieces:
-      T = t_setup + t_curl + 101 * t_matvec + sum_{j=0}^{99} (j + 2) * t_mgs_pair."""
+def oracle_rhs0(callback=None):
+    """The CPU oracle (numpy/scipy FP64 restatement of the reference path, all host cores) on right-hand side 0
+    of the workload: potential set-up, incident field, source term, b = G S, the complete GMRES solve as the
+    reference runs it (MGS, no restart, warm start b, maxiters = max(2 Bornmax, 100)), curl and crop.
+    ``callback(k)`` is called after GMRES iteration k.  Returns (result, start time, seconds)."""
     from oracle import cbs_oracle as O
-    import fmcuda as F
     med, _, srcs = make_inputs()
     t_pad = GRID[2] * RES[2]
     cfg = O.SolverConfig(RES, GRID, (O.PeriodicBC(), O.PeriodicBC(), O.AbsorbingBC(t_pad, t_pad, 1.0)))
     s = srcs[0]
     src = O.PlaneWave(WL, s.polarization, s.k_vector)
     t0 = time.perf_counter()
-    pot = O.build_potential(cfg, med.permittivity, EPS_BG, WL)
-    Ei, Hi = O.incident_field(src, cfg, EPS_BG)
-    S = pot.V[..., None] * Ei + (1j * pot.eps_imag) * Ei
-    b = O.green_conv(S, cfg, pot.k_square)
-    t_setup = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    for _ in range(2):
-        w = O.cbs_preconditioner(O.cbs_operator(b, pot.V, cfg, pot.k_square), pot.V, pot.eps_imag)
-    t_mv = (time.perf_counter() - t0) / 2
-    t0 = time.perf_counter()
-    for _ in range(8):
-        h = O._dot(b, w)
-        w = w - h * b
-    t_mgs = (time.perf_counter() - t0) / 8
-    t0 = time.perf_counter()
-    O.magnetic_field(b, RES, WL)
-    t_curl = time.perf_counter() - t0
-    iters = max(2 * pot.Bornmax, 100)
-    T = t_setup + t_curl + (iters + 1) * t_mv + sum((j + 2) * t_mgs for j in range(iters))
-    sample = (f"1 RHS of the workload: set-up + RHS, 2 operator applications, 8 MGS projections, 1 curl timed "
-              f"({t_setup:.2f}s, {t_mv:.2f}s/op, {t_mgs:.3f}s/proj); {iters}-iteration GMRES solve assembled "
-              f"from them")
-    return {"value": 1.0 / T, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port", "sample": sample,
-            "seconds_per_solve": T}
+    r = O.solve(cfg, src, med.permittivity, EPS_BG, callback=callback)
+    return r, t0, time.perf_counter() - t0
+
+
+def cpu_baseline():
+    """One complete oracle solve of right-hand side 0, timed on the host cores (see oracle_rhs0)."""
+    r, _, T = oracle_rhs0()
+    sample = (f"right-hand side 0 of the workload, one complete FP64 solve: set-up, RHS, {r.iterations} GMRES "
+              f"iterations (MGS), curl, crop; {T:.1f} s")
+    cb = {"value": 1.0 / T, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port", "sample": sample,
+          "seconds_per_solve": T, "iterations": r.iterations}
+    return cb, r
 
 
 def run_reference(args):
+    """The reference arm: the oracle (the CPU restatement of the reference's path; the reference itself is Julia,
+    which this image does not have) with all host cores.  Its steps are consecutive slices of complete solves of
+    right-hand side 0: step i is GMRES iterations (i*c, (i+1)*c] with c = ceil(maxiters / (warmup + steps)); the
+    first step of a solve also carries its set-up and the last its curl and crop.  ``value`` is one over the
+    duration of the complete solve(s); ``ms_per_step`` is the mean of the timed (non-warm-up) steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    vals = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline()
-        if i >= args.warmup:
-            vals.append(cb["value"])
-    v = statistics.median(vals)
-    cb["value"] = v
+    n_steps = args.warmup + args.steps
+    step_times = []        # duration of every step, over consecutive solves
+    solve_secs = []
+    iters_done = []
+    while len(step_times) < n_steps:
+        marks = []
+        r, t_start, T = oracle_rhs0(callback=lambda k: marks.append((k, time.perf_counter())))
+        c = max(1, math.ceil(r.iterations / n_steps))
+        ends = [t for k, t in marks if k % c == 0 and k < r.iterations] + [t_start + T]
+        starts = [t_start] + ends[:-1]
+        step_times += [e - b for b, e in zip(starts, ends)]
+        solve_secs.append(T)
+        iters_done.append(r.iterations)
+    timed = step_times[args.warmup:n_steps]
+    T = statistics.mean(solve_secs)
+    v = 1.0 / T
+    cb = {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+          "sample": f"right-hand side 0 of the workload, {len(solve_secs)} complete FP64 solve(s) of "
+                    f"{iters_done[0]} GMRES iterations split into {n_steps} steps; {T:.1f} s per solve",
+          "seconds_per_solve": T}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": "batching 128x128x64, 12 beads, 64 RHS (sample: 1 RHS per step)",
-                       "grid": list(GRID), "padded": [128, 128, 128], "rhs": 64, "solver": "gmres-100"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(timed),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": "batching: 128x128x64 (padded 128^3), 12 seeded beads, 64 RHS (32 NA-1.2 "
+                                   "angles x 2 pol), GMRES-100; sample: complete solves of RHS 0",
+                       "grid": list(GRID), "padded": [128, 128, 128], "rhs": 64, "solver": "gmres-100 (MGS)"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -187,6 +196,7 @@ def run_reference(args):
 def run(args):
     import torch
     import fmcuda as F
+    from fmcuda.replicas import max_over_ranks, shard
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -200,14 +210,18 @@ def run(args):
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
 
-    med, bcs, srcs = make_inputs()
-    srcs = srcs[: args.nrhs]
+    # The job: nrhs right-hand sides per GPU.  With N GPUs it has N*nrhs/2 angles x 2 polarisations, and every
+    # rank solves its own share of them (round-robin shard, weak scaling, no collective on the data path).
+    med, bcs, srcs_all = make_inputs(n_angles=world * args.nrhs // 2)
+    mine = shard(len(srcs_all), world, rank)
+    srcs = [srcs_all[i] for i in mine]
     lists = [[s] for s in srcs]
+    nrhs = len(lists)
     solver = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
                                     precision=args.precision,
                                     linear_solver=F.KrylovJL_GMRES(ortho=args.ortho, block_size=args.block,
                                                                    block_vectors=args.block_store),
-                                    max_rhs=args.nrhs, device_index=dev)
+                                    max_rhs=nrhs, device_index=dev)
     tuning = None
     if args.autotune:
         from fmcuda import autotune as AT
@@ -252,10 +266,8 @@ def run(args):
     launches = plan.launch_count() - launches0
     kstats = plan.kernel_stats()
     plan.set_profiling(False)
-    t_step = max(times)
-    from fmcuda.replicas import max_over_ranks
-    t_med = max_over_ranks(statistics.median(times))  # the slowest replica sets the job time
-    value = world * args.nrhs / t_med
+    t_med = max_over_ranks(statistics.median(times))  # the slowest rank sets the job time
+    value = world * nrhs / t_med
     n_pad = float(np.prod(solver.padded_size()))
     iters = [i.iterations for i in infos]
 
@@ -270,32 +282,48 @@ def run(args):
             outs = F.solve_batch(solver, lists, med)
             barrier()
             e2e_times.append(time.perf_counter() - t0)
-    e2e_t = statistics.median(e2e_times) if e2e_times else float("nan")
+    e2e_t = max_over_ranks(statistics.median(e2e_times)) if e2e_times else float("nan")
     g = int(np.prod(GRID))
     h2d = g * 16 + sum(GRID[d] + 2 * solver.padding()[d] for d in range(3)) * 8
-    d2h = 2 * args.nrhs * 3 * g * 16
+    d2h = 2 * nrhs * 3 * g * 16
 
     solver.release()  # the batched plan's device memory is not needed past this point
-    # plain FP64 GPU method (reference algorithm: GMRES with MGS, one RHS) and accuracy vs it
+    # The plain FP64 GPU method (the reference algorithm: GMRES with MGS, one RHS at a time), timed the same way
+    # as the batched form (CUDA events on the library stream, potential and fields resident in HBM), and end to
+    # end through F.solve (host permittivity in, host E/H out).
     fp64 = F.ConvergentBornSolver(resolution=RES, grid_size=GRID, boundary_conditions=bcs, tolerance=1e-6,
                                   precision="float64", linear_solver=F.KrylovJL_GMRES(ortho="mgs"), max_rhs=1,
                                   device_index=dev)
-    t64 = []
+    t64_dev, t64_e2e = [], []
+    ref = None
     with warnings.catch_warnings():
         warnings.simplefilter("ignore", RuntimeWarning)
         if args.fp64_steps > 0:
-            F.solve(fp64, srcs[0], med)  # untimed: plan creation and first-touch allocations
+            ref = F.solve(fp64, srcs[0], med)  # untimed: plan creation and first-touch allocations
+            p64 = fp64.plan()
+            o64 = fp64.solve_options(fp64.Bornmax)
+            s64 = torch.cuda.ExternalStream(p64.stream(), device=torch.device("cuda", dev))
+        for _ in range(args.fp64_steps):
+            barrier()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record(s64)
+            p64.solve_plane_waves(lists[:1], EPS_BG, o64, keep_on_device=True)
+            ev1.record(s64)
+            ev1.synchronize()
+            t64_dev.append(ev0.elapsed_time(ev1) / 1000.0)
         for _ in range(args.fp64_steps):
             barrier()
             t0 = time.perf_counter()
             ref = F.solve(fp64, srcs[0], med)
             barrier()
-            t64.append(time.perf_counter() - t0)
-    fp64_sps = 1.0 / statistics.median(t64) if t64 else float("nan")
+            t64_e2e.append(time.perf_counter() - t0)
+    fp64_sps = 1.0 / max_over_ranks(statistics.median(t64_dev)) if t64_dev else float("nan")
+    fp64_e2e_sps = 1.0 / max_over_ranks(statistics.median(t64_e2e)) if t64_e2e else float("nan")
     fp64_iters = fp64.iteration_count
     # accuracy of the batched form against the plain FP64 method on the first accuracy_rhs right-hand sides
     errs_e, errs_h = [], []
-    if t64 and outs:
+    if ref is not None and outs:
         errs_e.append(rel_l2(outs[0].E, ref.E))
         errs_h.append(rel_l2(outs[0].H, ref.H))
         with warnings.catch_warnings():
@@ -337,20 +365,31 @@ def run(args):
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args)
     cb = None
+    oracle_acc = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_baseline()
+        # the CPU oracle's complete FP64 solve of right-hand side 0: the CPU baseline, and the reference result
+        # both GPU forms are measured against
+        cb, orc = cpu_baseline()
+        oracle_acc = {"rhs": 0, "oracle_iterations": orc.iterations}
+        if outs:
+            oracle_acc.update(rel_l2_E_batched=rel_l2(outs[0].E, orc.E), rel_l2_H_batched=rel_l2(outs[0].H, orc.H))
+        if ref is not None:
+            oracle_acc.update(rel_l2_E_fp64=rel_l2(ref.E, orc.E), rel_l2_H_fp64=rel_l2(ref.H, orc.H),
+                              fp64_iterations=fp64_iters)
     clocks = clk.summary()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_med * 1000.0, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "c64", "data": "synthetic",
                 "config": {"workload": "batching: 128x128x64 (padded 128^3), 12 seeded beads, "
-                                       f"{args.nrhs} RHS (32 NA-1.2 angles x 2 pol), GMRES-{opts.maxiters}",
-                           "grid": list(GRID), "padded": list(solver.padded_size()), "rhs_per_gpu": args.nrhs,
+                                       f"{nrhs} RHS per GPU ({nrhs // 2} NA-1.2 angles x 2 pol), "
+                                       f"GMRES-{opts.maxiters}",
+                           "grid": list(GRID), "padded": list(solver.padded_size()), "rhs_per_gpu": nrhs,
+                           "rhs_total": world * nrhs,
                            "precision": f"{args.precision}: complex64 fields in HBM, FP64 dots"
                                         + (", FP64 FFT/Green/V arithmetic" if args.precision != "float32" else ""),
                            "ortho": args.ortho + (f"-{args.block}-{args.block_store}" if args.ortho == "block" else ""),
-                           "parallelism": f"replicas{world}",
+                           "parallelism": f"replicas{world}: right-hand sides sharded round-robin over ranks",
                            "l2": "inputs larger than L2 (Krylov basis of 50 MB vectors)", "seed": SEED,
                            "tuning": tuning},
                 "latency_s": {"p50": statistics.median(times), "p99": float(np.percentile(times, 99)),
@@ -360,11 +399,14 @@ def run(args):
                 "flops_model": {"per_iteration": 12 * 5 * n_pad * math.log2(n_pad),
                                 "achieved_GFLOPs": world * sum(iters) / t_med * 12 * 5 * n_pad * math.log2(n_pad) / 1e9,
                                 "model": "12 x 5 N log2 N per Born iteration (2 branches x fwd+inv x 3 components)"},
-                "fp64_plain": {"solves_per_s": fp64_sps, "iterations": fp64_iters,
+                "fp64_plain": {"solves_per_s": fp64_sps, "timing": "CUDA events, potential and fields in HBM",
+                               "e2e_solves_per_s": fp64_e2e_sps, "iterations": fp64_iters,
                                "rel_l2_E_fp32_vs_fp64": err_e, "rel_l2_H_fp32_vs_fp64": err_h,
                                "rel_l2_over_rhs": len(errs_e), "bar": 1e-5,
-                               "ratio_fp32_batched_over_fp64": value / world / fp64_sps},
-                "e2e": {"value": world * args.nrhs / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                               "ratio_fp32_batched_over_fp64": value / world / fp64_sps,
+                               "ratio_e2e": (world * nrhs / e2e_t) / world / fp64_e2e_sps},
+                "vs_oracle": oracle_acc,
+                "e2e": {"value": world * nrhs / e2e_t, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "roofline": roof, "kernel_classes": classes,
                 "algorithmic_GBps_all_kernels": all_bytes / (total_ms / 1000) / 1e9 if total_ms else None,

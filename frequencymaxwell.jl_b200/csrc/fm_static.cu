@@ -109,13 +109,16 @@ fm_status run(const fm_plan_desc& dsc, double k_bg, double eps_imag, int nrhs, c
     return noalloc_fail(FM_ERR_CUDA, std::string("table upload: ") + cudaGetErrorString(e));
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 148;
-  // physical units: k in 1/m, k_square = k_bg^2 + i eps_imag, inverse transforms normalised here
+  // k in units of k_bg (as the plans compute it), so |k|^2 - k_square stays O(1) in FP32 arithmetic:
+  // k' = k / k_bg, k_square' = k_square / k_bg^2, and G' = k_bg^2 G.  The factor 1 / k_bg^2 that returns the
+  // output to physical units is folded into the scale with the inverse-transform normalisation.
+  const double kref2 = k_bg * k_bg, kr = k_bg;
   GreenParams gp{};
-  for (int a = 0; a < 3; ++a) gp.dk[a] = 2.0 * M_PI / ((double)n3[a] * dsc.resolution[a]);
+  for (int a = 0; a < 3; ++a) gp.dk[a] = 2.0 * M_PI / ((double)n3[a] * dsc.resolution[a]) / kr;
   gp.shift[2] = zonly ? 0.25 : 0.0;
-  gp.ksq_re = k_bg * k_bg;
-  gp.ksq_im = eps_imag;
-  gp.scale_re = 1.0 / ((double)d.n * (zonly ? 2.0 : 1.0));
+  gp.ksq_re = 1.0;
+  gp.ksq_im = eps_imag / kref2;
+  gp.scale_re = 1.0 / ((double)d.n * (zonly ? 2.0 : 1.0) * kref2);
   const int mode = zonly ? ZMODE_AVG2 : ZMODE_ONE;
   void* tmp = sc + o_tmp;
   EpiParams ep{};

@@ -7,6 +7,7 @@ module FrequencyMaxwellCUDA
 
 using FrequencyMaxwell
 using KernelAbstractions
+using LinearAlgebra
 using LinearSolve
 
 const libfmcuda = get(ENV, "FMCUDA_LIB", joinpath(@__DIR__, "..", "fmcuda", "libfmcuda.so"))
@@ -220,6 +221,78 @@ function solve_fmcuda_batch(solver::ConvergentBornSolver{T}, sources_list, mediu
         ccall((:fm_plan_destroy, libfmcuda), Cvoid, (Ptr{Cvoid},), plan[])
     end
 end
+
+# ---- the operator and preconditioner for any LinearSolve.jl algorithm ---------------------------------
+# The device CBS operator (I - G_avg V) and left preconditioner (i/eps) V behind the reference's own
+# interfaces, so LinearSolve.jl algorithms other than the two that libfmcuda runs itself (e.g. IDRs,
+# BiCGStabL; docs/src/api.md:129-136) iterate on the device matvec:
+#
+#     A, Pl = fmcuda_operators(solver, medium, wavelength)
+#     sol = LinearSolve.solve(LinearProblem(A, b), IDRs(); Pl = Pl, reltol = 1e-6)
+#
+# Vectors are flattened (Nx', Ny', Nz', 3) fields on the padded grid, ComplexF64 on the host.
+
+"""Device plan with its potential, shared by the operator and the preconditioner below."""
+mutable struct FMCUDAPlan
+    ptr::Ptr{Cvoid}
+    n::Int               # 3 * padded voxels
+    bornmax::Int
+    function FMCUDAPlan(solver::ConvergentBornSolver, medium, wavelength)
+        desc = Ref(plan_desc(solver))
+        plan = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:fm_plan_create, libfmcuda), Cint, (Ref{FMPlanDesc}, Ref{Ptr{Cvoid}}), desc, plan))
+        p = new(plan[], 0, 0)
+        finalizer(q -> q.ptr == C_NULL || ccall((:fm_plan_destroy, libfmcuda), Cvoid, (Ptr{Cvoid},), q.ptr), p)
+        p.bornmax = build_potential!(p.ptr, solver, medium, wavelength)
+        d = desc[]
+        p.n = 3 * prod(Int(d.grid[i]) + 2 * Int(d.pad[i]) for i in 1:3)
+        return p
+    end
+end
+
+"""`CBSLinearOperator` (convergent_born.jl:452-518) on libfmcuda: y = beta*y + alpha*(x - G_avg(V.*x))."""
+struct FMCUDALinearOperator{T <: AbstractFloat}
+    plan::FMCUDAPlan
+end
+
+"""`CBSPreconditioner` (convergent_born.jl:379-431) on libfmcuda: y = (i/eps_imag) V.*x."""
+struct FMCUDAPreconditioner{T <: AbstractFloat}
+    plan::FMCUDAPlan
+end
+
+function fmcuda_operators(solver::ConvergentBornSolver{T}, medium, wavelength) where {T}
+    p = FMCUDAPlan(solver, medium, wavelength)
+    return FMCUDALinearOperator{T}(p), FMCUDAPreconditioner{T}(p)
+end
+
+function LinearAlgebra.mul!(y::AbstractVector, A::FMCUDALinearOperator, x::AbstractVector, α, β)
+    length(x) == A.plan.n == length(y) || throw(DimensionMismatch("operator is $(A.plan.n) x $(A.plan.n)"))
+    xc = Vector{ComplexF64}(x)
+    yc = Vector{ComplexF64}(y)
+    a, b = ComplexF64(α), ComplexF64(β)
+    check(ccall((:fm_apply_operator, libfmcuda), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{ComplexF64}, Ptr{ComplexF64}, Cdouble, Cdouble, Cdouble, Cdouble),
+                A.plan.ptr, Cint(1), xc, yc, real(a), imag(a), real(b), imag(b)))
+    y .= yc
+    return y
+end
+LinearAlgebra.mul!(y::AbstractVector, A::FMCUDALinearOperator, x::AbstractVector) = mul!(y, A, x, true, false)
+Base.:*(A::FMCUDALinearOperator{T}, x::AbstractVector) where {T} = mul!(similar(x, Complex{T}), A, x)
+Base.size(A::FMCUDALinearOperator) = (A.plan.n, A.plan.n)
+Base.size(A::FMCUDALinearOperator, dim::Integer) = size(A)[dim]
+Base.eltype(::FMCUDALinearOperator{T}) where {T} = Complex{T}
+Base.ndims(::FMCUDALinearOperator) = 2
+
+function LinearAlgebra.ldiv!(y::AbstractVector, P::FMCUDAPreconditioner, x::AbstractVector)
+    length(x) == P.plan.n == length(y) || throw(DimensionMismatch("preconditioner is $(P.plan.n) x $(P.plan.n)"))
+    xc = Vector{ComplexF64}(x)
+    yc = similar(xc)
+    check(ccall((:fm_apply_preconditioner, libfmcuda), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{ComplexF64}, Ptr{ComplexF64}), P.plan.ptr, Cint(1), xc, yc))
+    y .= yc
+    return y
+end
+LinearAlgebra.ldiv!(P::FMCUDAPreconditioner, x::AbstractVector) = ldiv!(x, P, copy(x))
 
 function __init__()
     FrequencyMaxwell.register_gpu_backend!(:fmcuda, () -> FMCUDABackend())

@@ -179,8 +179,9 @@ fm_status fm_synchronize(fm_plan* plan);
  * No counterpart in the reference (it solves one request per call).  An engine owns `slots` right-hand
  * sides on one plan; each slot holds one plane-wave right-hand side on its own permittivity, with its own
  * potential, eps_imag, Krylov basis of up to `basis` vectors and GMRES state (the reference's
- * KrylovJL_GMRES semantics per right-hand side: warm start b, no restart, maxiters = max(2*Bornmax, 100)
- * capped at `basis`, reltol = tolerance, abstol = tolerance*1e-2).  Requests share the engine's
+ * KrylovJL_GMRES semantics per right-hand side: warm start b, maxiters = max(2*Bornmax, 100), reltol =
+ * tolerance, abstol = tolerance*1e-2; when maxiters exceeds `basis` the slot restarts GMRES every `basis`
+ * iterations, i.e. it runs GMRES(basis), and full GMRES as the reference when maxiters fits the basis).  Requests share the engine's
  * wavelength, background permittivity and attenuation filters (fx, fy, fz over the padded axes, NULL =
  * ones) and take over the plan.  fm_engine_step admits queued right-hand sides into free slots, runs one
  * Krylov iteration on every running slot in shared launches (slots at different iterations), and

@@ -30,15 +30,38 @@ Manifest):
 """
 from __future__ import annotations
 
+import functools
 import math
 import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 import scipy.fft as sfft
+import threadpoolctl
 
 _WORKERS = os.cpu_count() or 1
+_POOL: Optional[ThreadPoolExecutor] = None
+
+
+def _slab_map(fn, nz: int) -> None:
+    """Run ``fn(z_slice)`` over contiguous z slabs on a thread pool.
+
+    The arithmetic per element is unchanged; numpy releases the GIL inside its loops, so
+    the slabs run in parallel.  Arrays are Fortran-ordered (x fastest), so a z slab of a
+    (nx, ny, nz[, 3]) array is a contiguous block (per component)."""
+    global _POOL
+    n = max(1, min(_WORKERS, nz))
+    bounds = [nz * i // n for i in range(n + 1)]
+    slabs = [slice(bounds[i], bounds[i + 1]) for i in range(n) if bounds[i + 1] > bounds[i]]
+    if n == 1:
+        fn(slabs[0])
+        return
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(_WORKERS)
+    for f in [_POOL.submit(fn, sl) for sl in slabs]:
+        f.result()
 
 # ----------------------------------------------------------------------------
 # Boundary conditions  (src/solvers/boundary_conditions.jl)
@@ -268,15 +291,27 @@ def curl_k_index(n: int) -> np.ndarray:
 
 
 def _fft3(a):
-    return sfft.fftn(a, axes=(0, 1, 2), workers=_WORKERS)
+    """Unnormalised 3-D DFT over the spatial axes (FFTW's forward ``fft``).  The transform runs on
+    the transposed (C-ordered) view so a Fortran-ordered input gives a Fortran-ordered output."""
+    nd = a.ndim
+    return sfft.fftn(a.T, axes=tuple(range(nd - 3, nd)), workers=_WORKERS).T
 
 
 def _ifft3(a):
-    return sfft.ifftn(a, axes=(0, 1, 2), workers=_WORKERS)
+    """1/N-normalised inverse 3-D DFT over the spatial axes (FFTW's ``ifft``)."""
+    nd = a.ndim
+    return sfft.ifftn(a.T, axes=tuple(range(nd - 3, nd)), workers=_WORKERS).T
 
 
 def phase_ramp(shape3, shifts, reverse: bool, dtype=np.complex128) -> np.ndarray:
     """multiply_phase_ramp_kernel! factor exp(-/+ 2*pi*i*sum_d (idx_d-1)*s_d/N_d) (dyadic_green.jl:243-266)."""
+    return _phase_ramp_cached(tuple(int(n) for n in shape3), tuple(float(s) for s in shifts), bool(reverse),
+                              np.dtype(dtype).str).copy(order="F")
+
+
+@functools.lru_cache(maxsize=16)
+def _phase_ramp_cached(shape3, shifts, reverse, dtype_str) -> np.ndarray:
+    dtype = np.dtype(dtype_str)
     ph = np.zeros(shape3)
     for d in range(3):
         if shifts[d] == 0:
@@ -286,62 +321,130 @@ def phase_ramp(shape3, shifts, reverse: bool, dtype=np.complex128) -> np.ndarray
         shp[d] = -1
         ph = ph + idx.reshape(shp)
     sgn = 1.0 if reverse else -1.0
-    return np.exp(sgn * 2j * np.pi * ph).astype(dtype)
+    out = np.asfortranarray(np.exp(sgn * 2j * np.pi * ph).astype(dtype))
+    out.flags.writeable = False
+    return out
+
+
+def _green_axes(shape3, freq_res, shifts, rdt):
+    kx = (freq_res[0] * (green_k_index(shape3[0]) + shifts[0])).astype(rdt).reshape(-1, 1, 1)
+    ky = (freq_res[1] * (green_k_index(shape3[1]) + shifts[1])).astype(rdt).reshape(1, -1, 1)
+    kz = (freq_res[2] * (green_k_index(shape3[2]) + shifts[2])).astype(rdt).reshape(1, 1, -1)
+    return kx, ky, kz
+
+
+def _green_multiply_into(src_hat: np.ndarray, out: np.ndarray, freq_res, shifts, k_square: complex) -> None:
+    """out <- Green(src_hat); ``out`` may be ``src_hat`` itself.  Same arithmetic as green_multiply."""
+    rdt = np.float64 if src_hat.dtype == np.complex128 else np.float32
+    kx, ky, kz = _green_axes(src_hat.shape[:3], freq_res, shifts, rdt)
+    ksq = src_hat.dtype.type(k_square)
+
+    def slab(sl):
+        kzs = kz[:, :, sl]
+        s1, s2, s3 = src_hat[:, :, sl, 0], src_hat[:, :, sl, 1], src_hat[:, :, sl, 2]
+        kE = (kx * s1 + ky * s2 + kzs * s3) / ksq
+        D = np.abs(kx * kx + ky * ky + kzs * kzs) - ksq
+        o1 = (s1 - kx * kE) / D
+        o2 = (s2 - ky * kE) / D
+        o3 = (s3 - kzs * kE) / D
+        out[:, :, sl, 0] = o1
+        out[:, :, sl, 1] = o2
+        out[:, :, sl, 2] = o3
+
+    _slab_map(slab, src_hat.shape[2])
 
 
 def green_multiply(src_hat: np.ndarray, freq_res, shifts, k_square: complex) -> np.ndarray:
-    """multiply_Green_kernel! (dyadic_green.jl:189-221).  k.E is divided by the complex k_square."""
-    nx, ny, nz = src_hat.shape[:3]
-    rdt = np.float64 if src_hat.dtype == np.complex128 else np.float32
-    kx = (freq_res[0] * (green_k_index(nx) + shifts[0])).astype(rdt).reshape(-1, 1, 1)
-    ky = (freq_res[1] * (green_k_index(ny) + shifts[1])).astype(rdt).reshape(1, -1, 1)
-    kz = (freq_res[2] * (green_k_index(nz) + shifts[2])).astype(rdt).reshape(1, 1, -1)
-    ksq = src_hat.dtype.type(k_square)
-    s1, s2, s3 = src_hat[..., 0], src_hat[..., 1], src_hat[..., 2]
-    kE = (kx * s1 + ky * s2 + kz * s3) / ksq
-    D = np.abs(kx * kx + ky * ky + kz * kz) - ksq
-    out = np.empty_like(src_hat)
-    out[..., 0] = (s1 - kx * kE) / D
-    out[..., 1] = (s2 - ky * kE) / D
-    out[..., 2] = (s3 - kz * kE) / D
+    """multiply_Green_kernel! (dyadic_green.jl:189-221).  k.E is divided by the complex k_square:
+    kE = (k . E)/k_sq, D = |k|^2 - k_sq, E_c <- (E_c - k_c kE)/D."""
+    out = np.empty(src_hat.shape, dtype=src_hat.dtype, order="F")
+    _green_multiply_into(src_hat, out, freq_res, shifts, k_square)
     return out
 
 
 def single_convolution(src: np.ndarray, cfg: SolverConfig, k_square: complex, shifts) -> np.ndarray:
-    """_apply_single_convolution! (dyadic_green.jl:161-179)."""
+    """_apply_single_convolution! (dyadic_green.jl:161-179): ramp(-), FFT, Green, IFFT, ramp(+)."""
     shape3 = src.shape[:3]
     freq_res = [2 * math.pi / (shape3[d] * cfg.resolution[d]) for d in range(3)]
     dt = src.dtype
-    x = src * phase_ramp(shape3, shifts, False, dt)[..., None]
-    x = _fft3(x).astype(dt)
-    x = green_multiply(x, freq_res, shifts, k_square)
-    x = _ifft3(x).astype(dt)
-    return x * phase_ramp(shape3, shifts, True, dt)[..., None]
+    shifted = any(s != 0 for s in shifts)
+    x = np.empty(src.shape, dtype=dt, order="F")
+    if shifted:
+        rf = _phase_ramp_cached(tuple(shape3), tuple(float(s) for s in shifts), False, np.dtype(dt).str)
+
+        def pre(sl):
+            for c in range(3):
+                np.multiply(src[:, :, sl, c], rf[:, :, sl], out=x[:, :, sl, c])
+        _slab_map(pre, shape3[2])
+    else:
+        x[...] = src
+    x = _fft3(x)
+    if x.dtype != dt:
+        x = x.astype(dt, order="F")
+    _green_multiply_into(x, x, freq_res, shifts, k_square)
+    x = _ifft3(x)
+    if x.dtype != dt:
+        x = x.astype(dt, order="F")
+    if shifted:
+        rr = _phase_ramp_cached(tuple(shape3), tuple(float(s) for s in shifts), True, np.dtype(dt).str)
+
+        def post(sl):
+            for c in range(3):
+                np.multiply(x[:, :, sl, c], rr[:, :, sl], out=x[:, :, sl, c])
+        _slab_map(post, shape3[2])
+    return x
 
 
 def green_conv(src: np.ndarray, cfg: SolverConfig, k_square: complex) -> np.ndarray:
     """conv!(::DyadicGreen, src) with the (G(+s) + G(-s))/2 average (dyadic_green.jl:127-152)."""
     shifts = cfg.shifts
+    src = np.asfortranarray(src)
     if not cfg.use_averaging:
         return single_convolution(src, cfg, k_square, shifts)
     a = single_convolution(src, cfg, k_square, shifts)
     b = single_convolution(src, cfg, k_square, tuple(-s for s in shifts))
-    return (a + b) / 2
+
+    def avg(sl):
+        a[:, :, sl] += b[:, :, sl]
+        a[:, :, sl] /= 2
+    _slab_map(avg, a.shape[2])
+    return a
+
+
+def _times_V(V: np.ndarray, x: np.ndarray, scale=None) -> np.ndarray:
+    """V .* x per component (times a scalar ``scale`` after the product when given)."""
+    x = np.asfortranarray(x)
+    out = np.empty(x.shape, dtype=np.result_type(V.dtype, x.dtype), order="F")
+
+    def slab(sl):
+        for c in range(3):
+            o = out[:, :, sl, c]
+            np.multiply(V[:, :, sl], x[:, :, sl, c], out=o)
+            if scale is not None:
+                o *= scale
+    _slab_map(slab, x.shape[2])
+    return out
 
 
 def cbs_operator(x: np.ndarray, V: np.ndarray, cfg: SolverConfig, k_square: complex,
                  alpha=1.0, beta=0.0, y: Optional[np.ndarray] = None) -> np.ndarray:
     """CBSLinearOperator: y = beta*y + alpha*(x - G_avg(V.*x)) (convergent_born.jl:482-508)."""
-    psi = green_conv(V[..., None] * x, cfg, k_square)
-    r = x - psi
-    if y is None or beta == 0:
-        return alpha * r
-    return beta * y + alpha * r
+    x = np.asfortranarray(x)
+    psi = green_conv(_times_V(V, x), cfg, k_square)
+
+    def slab(sl):
+        r = x[:, :, sl] - psi[:, :, sl]
+        if y is None or beta == 0:
+            psi[:, :, sl] = alpha * r if alpha != 1.0 else r
+        else:
+            psi[:, :, sl] = beta * y[:, :, sl] + alpha * r
+    _slab_map(slab, x.shape[2])
+    return psi
 
 
 def cbs_preconditioner(x: np.ndarray, V: np.ndarray, eps_imag: float) -> np.ndarray:
     """CBSPreconditioner ldiv!: y = (i/eps_imag) .* V .* x (convergent_born.jl:398-431)."""
-    return (V[..., None] * x) * (1j / eps_imag)
+    return _times_V(V, x, 1j / eps_imag)
 
 
 # ----------------------------------------------------------------------------
@@ -356,14 +459,88 @@ class KrylovResult:
     residuals: List[float] = field(default_factory=list)
 
 
+def _chunks(n: int):
+    k = max(1, min(_WORKERS, n // 65536))
+    b = [n * i // k for i in range(k + 1)]
+    return [slice(b[i], b[i + 1]) for i in range(k)]
+
+
+def _pool_map(fn, items):
+    global _POOL
+    if len(items) == 1:
+        return [fn(items[0])]
+    if _POOL is None:
+        _POOL = ThreadPoolExecutor(_WORKERS)
+    return [f.result() for f in [_POOL.submit(fn, it) for it in items]]
+
+
 def _dot(a, b) -> complex:
-    """Julia dot(a, b) = sum(conj(a) .* b), accumulated in complex128."""
-    return complex(np.vdot(a.astype(np.complex128, copy=False).ravel(order="K"),
-                           b.astype(np.complex128, copy=False).ravel(order="K")))
+    """Julia dot(a, b) = sum(conj(a) .* b), accumulated in complex128 (chunk partial sums added in
+    chunk order)."""
+    a = a.astype(np.complex128, copy=False)
+    b = b.astype(np.complex128, copy=False)
+    if a.strides != b.strides or not a.flags.f_contiguous:
+        a, b = np.asfortranarray(a), np.asfortranarray(b)
+    ar, br = a.ravel(order="K"), b.ravel(order="K")
+    parts = _pool_map(lambda sl: complex(np.vdot(ar[sl], br[sl])), _chunks(ar.size))
+    tot = 0j
+    for p in parts:
+        tot += p
+    return tot
 
 
 def _nrm(a) -> float:
     return float(np.sqrt(np.real(_dot(a, a))))
+
+
+_BLK = 1 << 17
+
+
+def _axpy_block(a, xs, ys, tmp) -> None:
+    """ys <- ys + a*xs on one block (numpy loops release the GIL, so blocks run in parallel)."""
+    t = tmp[:ys.size]
+    np.multiply(xs, a, out=t)
+    np.add(ys, t, out=ys)
+
+
+def _axpy_dot(a: complex, xv: np.ndarray, yv: np.ndarray, zv: np.ndarray) -> complex:
+    """One fused modified Gram-Schmidt stage: yv <- yv + a*xv, then return dot(zv, yv).
+
+    Per element the arithmetic is that of the two separate steps; the pass runs in cache-sized
+    blocks so yv is read once for both.  All three arrays are complex128 with equal strides."""
+    xr, yr, zr = xv.ravel(order="K"), yv.ravel(order="K"), zv.ravel(order="K")
+    a = complex(a)
+
+    def part(sl):
+        tmp = np.empty(_BLK, dtype=np.complex128)
+        tot = 0j
+        for s0 in range(sl.start, sl.stop, _BLK):
+            b = slice(s0, min(s0 + _BLK, sl.stop))
+            _axpy_block(a, xr[b], yr[b], tmp)
+            tot += complex(np.vdot(zr[b], yr[b]))
+        return tot
+    parts = _pool_map(part, _chunks(yr.size))
+    tot = 0j
+    for p in parts:
+        tot += p
+    return tot
+
+
+def _axpy(a: complex, xv: np.ndarray, yv: np.ndarray) -> None:
+    """yv <- yv + a*xv in place."""
+    if (yv.dtype == xv.dtype and yv.shape == xv.shape and yv.strides == xv.strides
+            and (yv.flags.f_contiguous or yv.flags.c_contiguous)):
+        xr, yr = xv.ravel(order="K"), yv.ravel(order="K")
+        av = yv.dtype.type(a)
+
+        def part(sl):
+            tmp = np.empty(_BLK, dtype=yv.dtype)
+            for s0 in range(sl.start, sl.stop, _BLK):
+                b = slice(s0, min(s0 + _BLK, sl.stop))
+                _axpy_block(av, xr[b], yr[b], tmp)
+        _pool_map(part, _chunks(yr.size))
+        return
+    yv += yv.dtype.type(a) * xv
 
 
 def sym_givens(a: complex, b: float):
@@ -381,14 +558,36 @@ def sym_givens(a: complex, b: float):
 
 
 def gmres(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
-          itmax: int, restart: int = 0) -> KrylovResult:
+          itmax: int, restart: int = 0, callback=None) -> KrylovResult:
+    """Left-preconditioned GMRES of Krylov.jl (see ``_gmres_impl``).  ``callback(k)``, when given,
+    is called after inner iteration k (1-based, counted over restarts)."""
+    with threadpoolctl.threadpool_limits(1, user_api="blas"):
+        return _gmres_impl(apply_A, apply_M, b, x0, atol, rtol, itmax, restart, callback)
+
+
+def bicgstab(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
+             itmax: int) -> KrylovResult:
+    """Left-preconditioned BiCGStab of Krylov.jl (see ``_bicgstab_impl``)."""
+    with threadpoolctl.threadpool_limits(1, user_api="blas"):
+        return _bicgstab_impl(apply_A, apply_M, b, x0, atol, rtol, itmax)
+
+
+def richardson(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
+               itmax: int) -> KrylovResult:
+    """The plain convergent Born series (see ``_richardson_impl``)."""
+    with threadpoolctl.threadpool_limits(1, user_api="blas"):
+        return _richardson_impl(apply_A, apply_M, b, x0, atol, rtol, itmax)
+
+
+def _gmres_impl(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
+                itmax: int, restart: int = 0, callback=None) -> KrylovResult:
     """Left-preconditioned GMRES with warm start, as Krylov.jl ``gmres`` runs it under LinearSolve
     (``KrylovJL_GMRES``: ``restart=false`` -> full GMRES whose basis grows; MGS; Givens).
 
     ``restart > 0`` gives GMRES(m) (restart every m inner iterations, x kept).
     Residual = M^{-1}(b - A x); stop when its estimate <= atol + rtol*||r0||.
     """
-    x = x0.copy()
+    x = np.asfortranarray(x0).copy(order="F")
     r0 = apply_M(b - apply_A(x))
     beta = _nrm(r0)
     rnorms = [beta]
@@ -412,10 +611,20 @@ def gmres(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: fl
             inner += 1
             q = apply_M(apply_A(Vb[-1]))
             col = []
+            q = np.asfortranarray(q)
+            fused = q.dtype == np.complex128 and all(v.strides == q.strides and v.dtype == q.dtype for v in Vb)
             for i in range(inner):
-                h = _dot(Vb[i], q)
+                # modified Gram-Schmidt: h_i = <v_i, q>; q <- q - h_i v_i (the update of stage i-1 and
+                # the dot of stage i share one pass over q when the layouts allow it)
+                if i == 0 or not fused:
+                    h = _dot(Vb[i], q)
+                else:
+                    h = _axpy_dot(-col[-1], Vb[i - 1], q, Vb[i])
                 col.append(h)
-                q = q - h * Vb[i]
+                if not fused:
+                    _axpy(-h, Vb[i], q)
+            if fused:
+                _axpy(-col[-1], Vb[inner - 1], q)
             hb = _nrm(q)
             for i in range(inner - 1):
                 t = cs[i] * col[i] + ss[i] * col[i + 1]
@@ -430,6 +639,8 @@ def gmres(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: fl
             z[inner - 1] = c * z[inner - 1]
             rnorm = abs(zk1)
             rnorms.append(rnorm)
+            if callback is not None:
+                callback(it + inner)
             solved = rnorm <= eps or (rnorm + 1.0 <= 1.0)
             breakdown = hb <= btol
             tired = (it + inner) >= itmax or inner >= m
@@ -446,16 +657,17 @@ def gmres(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: fl
                 y[: i + 1] = [0j] * (i + 1)
                 break
             y[i] = y[i] / H[i][i]
+        x = np.asfortranarray(x)
         for i in range(inner):
-            x = x + y[i] * Vb[i]
+            _axpy(y[i], Vb[i], x)
         it += inner
         if breakdown:
             break
     return KrylovResult(x, it, bool(solved), rnorms)
 
 
-def bicgstab(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
-             itmax: int) -> KrylovResult:
+def _bicgstab_impl(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
+                   itmax: int) -> KrylovResult:
     """Left-preconditioned BiCGStab (van der Vorst 1992) in the form of Krylov.jl ``bicgstab``:
     warm start solves A dx = b - A x0, shadow vector c = b, residual r = M^{-1}(b - A x)."""
     r0 = b - apply_A(x0)
@@ -496,8 +708,8 @@ def bicgstab(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol:
     return KrylovResult(x0 + dx, it, bool(solved), rnorms)
 
 
-def richardson(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
-               itmax: int) -> KrylovResult:
+def _richardson_impl(apply_A, apply_M, b: np.ndarray, x0: np.ndarray, atol: float, rtol: float,
+                     itmax: int) -> KrylovResult:
     """Plain convergent Born series: x <- x + M^{-1}(b - A x), with the same stopping rule as the
     Krylov forms (||M^{-1}(b - A x)|| <= atol + rtol*||M^{-1}(b - A x0)||)."""
     x = x0.copy()
@@ -709,8 +921,10 @@ class SolveResult:
 def solve(cfg: SolverConfig, sources, permittivity: np.ndarray, permittivity_bg: float,
           dtype=np.complex128, method: Optional[str] = None, restart: int = 0,
           atol: Optional[float] = None, rtol: Optional[float] = None,
-          itmax: Optional[int] = None) -> SolveResult:
-    """LinearSolve.solve(::ConvergentBornSolver, sources, medium) (convergent_born.jl:565-600)."""
+          itmax: Optional[int] = None, callback=None) -> SolveResult:
+    """LinearSolve.solve(::ConvergentBornSolver, sources, medium) (convergent_born.jl:565-600).
+
+    ``callback(k)`` is passed to GMRES (called after each iteration k)."""
     method = method or cfg.method
     wl = source_wavelength(sources)
     pot = build_potential(cfg, permittivity, permittivity_bg, wl, dtype)
@@ -721,14 +935,14 @@ def solve(cfg: SolverConfig, sources, permittivity: np.ndarray, permittivity_bg:
         raise RuntimeError("Bornmax < 1: the reference leaves the field undefined")
     ksq = pot.k_square
     b = green_conv(S.astype(dtype), cfg, ksq)                               # :720-728
-    x0 = b.copy()
+    x0 = b.copy(order="F")
     A = lambda v: cbs_operator(v, V, cfg, ksq)
-    M = lambda v: cbs_preconditioner(v, V, pot.eps_imag).astype(dtype)
+    M = lambda v: cbs_preconditioner(v, V, pot.eps_imag).astype(dtype, copy=False)
     rt = cfg.tolerance if rtol is None else rtol
     at = cfg.tolerance * 1e-2 if atol is None else atol                    # :743-747
     mi = max(pot.Bornmax * 2, 100) if itmax is None else itmax
     if method == "gmres":
-        res = gmres(A, M, b, x0, at, rt, mi, restart)
+        res = gmres(A, M, b, x0, at, rt, mi, restart, callback)
     elif method == "bicgstab":
         res = bicgstab(A, M, b, x0, at, rt, mi)
     elif method == "richardson":
