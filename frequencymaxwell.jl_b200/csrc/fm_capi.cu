@@ -19,6 +19,7 @@
 #include "../../include/fmcuda.h"
 #include "fm_blockdot.h"
 #include "fm_krylov.cuh"
+#include "fm_generic.h"
 #include "fm_launch.h"
 #include "fm_setup.cuh"
 #include "fm_tables.h"
@@ -94,6 +95,9 @@ struct fm_plan {
   bool avg = false;     // any absorbing axis
   bool zonly = false;   // shifts only on z -> single pass with the length-2L transform
   bool zsplit = false;  // shifts only on z, padded z longer than the length-2L pass takes: two z passes
+  bool generic = false; // an axis without a fused pass (fm_generic.cuh): plain passes, Bluestein where needed
+  GenAxis gax[3];       // device tables of the general passes per axis
+  DevBuf gtw[3], gch[3][2], gkn[3][2];
   double shift[3] = {0, 0, 0};
   // potential / physics
   bool have_pot = false;
@@ -103,7 +107,7 @@ struct fm_plan {
   DevBuf twx, twy, twz, twz2, rz, rxp, rxm, ryp, rym, rzp, rzm;
   DevBuf V;
   // workspace
-  DevBuf t1, t2, bbuf, xbuf, ebuf, sbuf, basis, gbuf2;
+  DevBuf t1, t2, t3, bbuf, xbuf, ebuf, sbuf, basis, gbuf2;  // t3: first branch of a two-branch average
   DevBuf red_part, red_out, red_cnt, active, scale, coef, hbuf, shifts, yblk, V64;
   DevBuf eps_dev, fx, fy, fz, maxpart, maxout;
   DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
@@ -259,6 +263,34 @@ static cudaError_t upload_cplx(DevBuf& buf, const std::vector<cd>& v, cudaStream
 
 template <typename R>
 static fm_status init_tables(fm_plan* P) {
+  if (P->generic) {
+    const int n3[3] = {P->dims.nx, P->dims.ny, P->dims.nz};
+    for (int a = 0; a < 3; ++a) {
+      const GenAxisTables t = gen_axis_tables(n3[a]);
+      GenAxis& g = P->gax[a];
+      g.n = t.n;
+      g.m = t.m;
+      FM_CK(upload_cplx<R>(P->gtw[a], twiddles<R>(t.m), P->st));
+      g.tw = P->gtw[a].p;
+      if (t.m != t.n) {
+        for (int dir = 0; dir < 2; ++dir) {
+          FM_CK(upload_cplx<R>(P->gch[a][dir], t.chirp[dir], P->st));
+          FM_CK(upload_cplx<R>(P->gkn[a][dir], t.kern[dir], P->st));
+          g.chirp[dir] = P->gch[a][dir].p;
+          g.kern[dir] = P->gkn[a][dir].p;
+        }
+      }
+    }
+    if (P->avg) {
+      FM_CK(upload_cplx<R>(P->rxp, ramp(P->dims.nx, P->shift[0], -1.0), P->st));
+      FM_CK(upload_cplx<R>(P->rxm, ramp(P->dims.nx, P->shift[0], +1.0), P->st));
+      FM_CK(upload_cplx<R>(P->ryp, ramp(P->dims.ny, P->shift[1], -1.0), P->st));
+      FM_CK(upload_cplx<R>(P->rym, ramp(P->dims.ny, P->shift[1], +1.0), P->st));
+      FM_CK(upload_cplx<R>(P->rzp, ramp(P->dims.nz, P->shift[2], -1.0), P->st));
+      FM_CK(upload_cplx<R>(P->rzm, ramp(P->dims.nz, P->shift[2], +1.0), P->st));
+    }
+    return FM_OK;
+  }
   FM_CK(upload_cplx<R>(P->twx, twiddles<R>(P->dims.nx), P->st));
   FM_CK(upload_cplx<R>(P->twy, twiddles<R>(P->dims.ny), P->st));
   FM_CK(upload_cplx<R>(P->twz, twiddles<R>(P->dims.nz), P->st));
@@ -330,11 +362,121 @@ struct RhsCtx {
   VecTab vt;
 };
 
+// ---------------------------------------------------------------------------
+// General-length path (fm_generic.cuh): plain passes, one or two branches
+// ---------------------------------------------------------------------------
+template <typename S>
+static cudaError_t gen_axis(const fm_plan* P, const Dims& d, int axis, int dir, void* f, const int* act) {
+  if constexpr (std::is_same<S, double>::value)
+    return launch_gen_axis<double, double>(d, axis, dir, f, f, P->gax[axis], act, P->st);
+  else return P->c64 ? launch_gen_axis<float, double>(d, axis, dir, f, f, P->gax[axis], act, P->st)
+                     : launch_gen_axis<float, float>(d, axis, dir, f, f, P->gax[axis], act, P->st);
+}
+template <typename S>
+static cudaError_t gen_pre(const fm_plan* P, const Dims& d, int pro, const void* in, const void* V, const double* rs,
+                           const GenRamps& rp, void* out, const int* act, VecTab vt) {
+  if constexpr (std::is_same<S, double>::value)
+    return launch_gen_pre<double, double>(d, pro, in, V, rs, rp, out, act, P->st, vt);
+  else return P->c64 ? launch_gen_pre<float, double>(d, pro, in, V, rs, rp, out, act, P->st, vt)
+                     : launch_gen_pre<float, float>(d, pro, in, V, rs, rp, out, act, P->st, vt);
+}
+template <typename S>
+static cudaError_t gen_kspace(const fm_plan* P, const Dims& d, int mode, void* f, const GreenParams& gp, const int* act) {
+  if constexpr (std::is_same<S, double>::value) return launch_gen_kspace<double, double>(d, mode, f, gp, act, P->st);
+  else return P->c64 ? launch_gen_kspace<float, double>(d, mode, f, gp, act, P->st)
+                     : launch_gen_kspace<float, float>(d, mode, f, gp, act, P->st);
+}
+template <typename S>
+static cudaError_t gen_post(const fm_plan* P, const Dims& d, int epi, const void* in, const void* V, const void* xv,
+                            const void* bv, const double* rs, const EpiParams& ep, const GenRamps& rp, void* out,
+                            const int* act, VecTab vt) {
+  if constexpr (std::is_same<S, double>::value)
+    return launch_gen_post<double, double>(d, epi, in, V, xv, bv, rs, ep, rp, out, act, P->st, vt);
+  else return P->c64 ? launch_gen_post<float, double>(d, epi, in, V, xv, bv, rs, ep, rp, out, act, P->st, vt)
+                     : launch_gen_post<float, float>(d, epi, in, V, xv, bv, rs, ep, rp, out, act, P->st, vt);
+}
+
+// The Green application / CBS operator of green_op on a plan with an axis that has no fused pass.  Per branch:
+// PRE (potential, forward ramps) -> forward DFT along x, y, z -> Green of the branch -> inverse DFT along z, y,
+// x -> POST (reverse ramps, epilogue).  With an absorbing axis the +s branch stores half its result in t3 and
+// the -s branch adds it before the epilogue (dyadic_green.jl:127-152).
+template <typename R>
+static fm_status gen_green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
+                              const void* bv, const EpiParams& ep_in, void* out, const int* act, int nact,
+                              const RhsCtx* rc) {
+  using T = cplx<R>;
+  if (nact < 0) nact = nb;
+  EpiParams ep = ep_in;
+  if (rc) ep.inv_eps_b = rc->inv_eps_b;
+  Dims d = P->dims;
+  d.nb = nb;
+  const size_t fbytes = (size_t)nb * P->M * sizeof(T);
+  const double fbA = (double)nact * P->M * sizeof(T), vb = (double)nact * P->n * sizeof(T);
+  FM_CK(P->t1.ensure(fbytes));
+  const int nbr = P->avg ? 2 : 1;
+  if (nbr == 2) FM_CK(P->t3.ensure(fbytes));
+  GreenParams gp{};
+  const double kr = std::sqrt(P->kref2);
+  for (int a = 0; a < 3; ++a) gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]) / kr;
+  gp.ksq_re = P->k_bg * P->k_bg / P->kref2;
+  gp.ksq_im = P->eps_imag / P->kref2;
+  gp.scale_re = 1.0 / ((double)P->n * nbr);
+  const void* V = P->V.p;
+  VecTab vt{};
+  if (rc) {
+    V = rc->V;
+    d.vstride = rc->vstride;
+    gp.ksq_im_b = rc->ksq_im_b;
+    vt = rc->vt;
+  }
+  double postb = 2 * fbA;
+  if (epi != EPI_STORE) postb += fbA;
+  if (epi == EPI_PREC_RES) postb += fbA;
+  if (epi == EPI_PREC_OP || epi == EPI_PREC_RES) postb += vb;
+  if (epi == EPI_OP && (ep.beta_re != 0.0 || ep.beta_im != 0.0)) postb += fbA;
+  const DevBuf* rpos[3] = {&P->rxp, &P->ryp, &P->rzp};
+  const DevBuf* rneg[3] = {&P->rxm, &P->rym, &P->rzm};
+  cudaError_t e;
+  for (int br = 0; br < nbr; ++br) {
+    GenRamps rp;
+    for (int a = 0; a < 3; ++a) {
+      gp.shift[a] = (br == 0 ? 1.0 : -1.0) * P->shift[a];
+      rp.r[a] = P->shift[a] != 0.0 ? (br == 0 ? rpos[a]->p : rneg[a]->p) : nullptr;
+    }
+    FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
+             e = gen_pre<R>(P, d, pro, in, V, rs, rp, P->t1.p, act, vt));
+    FM_CK(e);
+    for (int a = 0; a < 3; ++a) {
+      FM_TRACK(P, KC_YF, 2 * fbA, e = gen_axis<R>(P, d, a, -1, P->t1.p, act));
+      FM_CK(e);
+    }
+    FM_TRACK(P, KC_ZG, 2 * fbA, e = gen_kspace<R>(P, d, ZMODE_ONE, P->t1.p, gp, act));
+    FM_CK(e);
+    for (int a = 2; a >= 0; --a) {
+      FM_TRACK(P, KC_YI, 2 * fbA, e = gen_axis<R>(P, d, a, +1, P->t1.p, act));
+      FM_CK(e);
+    }
+    if (nbr == 2 && br == 0) {
+      EpiParams e0{};
+      FM_TRACK(P, KC_XI, 2 * fbA,
+               e = gen_post<R>(P, d, EPI_STORE, P->t1.p, V, nullptr, nullptr, nullptr, e0, rp, P->t3.p, act, VecTab{}));
+    } else {
+      EpiParams e1 = ep;
+      if (nbr == 2) e1.gadd = P->t3.p;
+      FM_TRACK(P, KC_XI, postb + (nbr == 2 ? fbA : 0.0),
+               e = gen_post<R>(P, d, epi, P->t1.p, V, xv, bv, rs, e1, rp, out, act, vt));
+    }
+    FM_CK(e);
+  }
+  return FM_OK;
+}
+
 template <typename R>
 static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
                           const void* bv, const EpiParams& ep_in, void* out, const int* act, int nact = -1,
                           const RhsCtx* rc = nullptr) {
   using T = cplx<R>;
+  if (P->generic) return gen_green_op<R>(P, nb, in, pro, rs, epi, xv, bv, ep_in, out, act, nact, rc);
   if (nact < 0) nact = nb;
   EpiParams ep = ep_in;
   if (rc) ep.inv_eps_b = rc->inv_eps_b;
@@ -405,8 +547,45 @@ static fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const dou
     FM_CK(e);
     return FM_OK;
   }
-  // general case (sub-pixel shifts on x or y): the two branches run separately and are averaged
-  return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build (only z)");
+  // General case: sub-pixel shifts on x or y (absorbing x or y boundaries).  The branches G(+s) and G(-s)
+  // (dyadic_green.jl:127-152) differ on every shifted axis, so each runs its own five passes with its phase
+  // ramps (dyadic_green.jl:243-266, per axis: x in the x passes, y in the y passes, z in the z pass) and its
+  // shifted k (dyadic_green.jl:189-221).  Branch + stores half of G(+s) psi in t3; branch - adds it to half of
+  // G(-s) psi in the XI pass, before the epilogue.
+  {
+    FM_CK(P->t3.ensure(fbytes));
+    gp.scale_re = 1.0 / ((double)P->n * 2.0);
+    cudaError_t e;
+    for (int br = 0; br < 2; ++br) {
+      const double sg = br == 0 ? 1.0 : -1.0;
+      for (int a = 0; a < 3; ++a) gp.shift[a] = sg * P->shift[a];
+      const void* rx = P->shift[0] != 0.0 ? (br == 0 ? P->rxp.p : P->rxm.p) : nullptr;
+      const void* ry = P->shift[1] != 0.0 ? (br == 0 ? P->ryp.p : P->rym.p) : nullptr;
+      const void* rzt = P->shift[2] != 0.0 ? (br == 0 ? P->rzp.p : P->rzm.p) : nullptr;
+      FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
+               e = pass_xf<R>(P, d, pro, in, V, rs, P->twx.p, rx, P->t1.p, act, vt));
+      FM_CK(e);
+      FM_TRACK(P, KC_YF, 2 * fbA, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, ry, P->t2.p, act));
+      FM_CK(e);
+      FM_TRACK(P, KC_ZG, 2 * fbA, e = pass_zg<R>(P, d, ZMODE_ONE, P->t2.p, gp, P->twz.p, rzt, P->t1.p, act));
+      FM_CK(e);
+      FM_TRACK(P, KC_YI, 2 * fbA, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, ry, P->t2.p, act));
+      FM_CK(e);
+      if (br == 0) {
+        EpiParams e0{};
+        FM_TRACK(P, KC_XI, 2 * fbA,
+                 e = pass_xi<R>(P, d, EPI_STORE, P->t2.p, V, nullptr, nullptr, nullptr, e0, P->twx.p, rx, P->t3.p,
+                                act));
+      } else {
+        EpiParams e1 = ep;
+        e1.gadd = P->t3.p;
+        FM_TRACK(P, KC_XI, xib + fbA,
+                 e = pass_xi<R>(P, d, epi, P->t2.p, V, xv, bv, rs, e1, P->twx.p, rx, out, act, vt));
+      }
+      FM_CK(e);
+    }
+    return FM_OK;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1596,6 +1775,25 @@ static fm_status curl_batch(fm_plan* P, int nb, const void* in, void* out, const
   gp.scale_im = -f;
   const double cb = 2.0 * nb * P->M * sizeof(T);
   cudaError_t e;
+  if (P->generic) {
+    GenRamps none;
+    FM_TRACK(P, KC_CURL, cb, e = gen_pre<R>(P, d, PRO_COPY, in, nullptr, nullptr, none, P->t1.p, act, VecTab{}));
+    FM_CK(e);
+    for (int a = 0; a < 3; ++a) {
+      FM_TRACK(P, KC_CURL, cb, e = gen_axis<R>(P, d, a, -1, P->t1.p, act));
+      FM_CK(e);
+    }
+    FM_TRACK(P, KC_CURL, cb, e = gen_kspace<R>(P, d, ZMODE_CURL, P->t1.p, gp, act));
+    FM_CK(e);
+    for (int a = 2; a >= 0; --a) {
+      FM_TRACK(P, KC_CURL, cb, e = gen_axis<R>(P, d, a, +1, P->t1.p, act));
+      FM_CK(e);
+    }
+    FM_TRACK(P, KC_CURL, cb,
+             e = gen_post<R>(P, d, EPI_STORE, P->t1.p, nullptr, nullptr, nullptr, nullptr, ep, none, out, act, VecTab{}));
+    FM_CK(e);
+    return FM_OK;
+  }
   FM_TRACK(P, KC_CURL, cb, e = pass_xf<R>(P, d, PRO_COPY, in, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, act));
   FM_CK(e);
   FM_TRACK(P, KC_CURL, cb, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
@@ -1710,8 +1908,11 @@ static fm_status plan_wave_size(fm_plan* P, int nrhs, const fm_solve_opts& o, in
   else vecs = 1;
   // basis + b + x + s + e + t1 + t2 + fp64 staging and outputs
   // (the output term also covers the second output slot of host-output solves: 2 * 3g * 16 <= 2 * M * 16)
-  const size_t per = fb * (size_t)(vecs + 6) + (size_t)P->M * sizeof(double2) * 5 + extra;
+  // (+ t3 when the Green average runs as two branches: absorbing x or y)
+  const size_t two_branch = (P->avg && !P->zonly && !P->zsplit) ? 1 : 0;  // (the general passes use t1 and t3)
+  const size_t per = fb * (size_t)(vecs + 6 + two_branch) + (size_t)P->M * sizeof(double2) * 5 + extra;
   const size_t held = P->basis.cap + P->bbuf.cap + P->xbuf.cap + P->sbuf.cap + P->ebuf.cap + P->t1.cap + P->t2.cap +
+                      P->t3.cap +
                       P->gbuf2.cap + P->Eo.cap + P->Ho.cap + P->yblk.cap;
   const size_t avail = (size_t)((freeb + held) * 0.92);
   wave = (int)std::max<size_t>(1, std::min<size_t>((size_t)nrhs, avail / per));
@@ -1761,23 +1962,30 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) return fail(FM_ERR_CUDA, "no CUDA device");
   if (desc->device < 0 || desc->device >= nd) return fail(FM_ERR_INVALID, "device ordinal out of range");
   const int n3[3] = {desc->grid[0] + 2 * desc->pad[0], desc->grid[1] + 2 * desc->pad[1], desc->grid[2] + 2 * desc->pad[2]};
-  for (int a = 0; a < 3; ++a)
-    if (!axis_supported(n3[a]))
-      return fail(FM_ERR_UNSUPPORTED, "padded axis sizes must be 96 or powers of two in [8, 512] in this build");
   bool avg = desc->absorbing[0] || desc->absorbing[1] || desc->absorbing[2];
   bool zonly = desc->absorbing[2] && !desc->absorbing[0] && !desc->absorbing[1];
-  if (avg && !zonly) return fail(FM_ERR_UNSUPPORTED, "absorbing boundaries on x or y are not supported by this build");
-  if (zonly && (n3[2] > AXIS_MAX || (n3[2] & (n3[2] - 1))))
-    return fail(FM_ERR_UNSUPPORTED,
-                "an absorbing z boundary needs a power-of-two padded z size of at most 512 in this build");
-  // padded z above 256: the two shifted branches run as two z passes (the second adds to the first)
-  const bool zsplit = zonly && n3[2] > AXIS_MAX_AVG2;
   const int prec = desc->precision == FM_PREC_F64 ? FM_PREC_F64 : FM_PREC_F32;  // storage
   const bool c64 = desc->precision != FM_PREC_F32;                                   // arithmetic
-  const int pwy = c64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
-  const int lz = (zonly && !zsplit) ? 2 * n3[2] : n3[2];
-  const int pwz = c64 ? pencils_per_warp<double>(lz) : pencils_per_warp<float>(lz);
-  if (pwy <= 0 || pwz <= 0 || n3[0] % pwy || n3[0] % pwz) return fail(FM_ERR_UNSUPPORTED, "x size too small for pencil tiling");
+  // The fused passes take axes of 96 or powers of two in [8, 512] (an averaged z axis a power of two) that
+  // tile the warps; every other grid runs the general passes (fm_generic.cuh).
+  bool generic = false;
+  for (int a = 0; a < 3; ++a)
+    if (!axis_supported(n3[a])) generic = true;
+  if (zonly && (n3[2] > AXIS_MAX || (n3[2] & (n3[2] - 1)))) generic = true;
+  // padded z above 256: the two shifted branches run as two z passes (the second adds to the first)
+  bool zsplit = zonly && n3[2] > AXIS_MAX_AVG2;
+  if (!generic) {
+    const int pwy = c64 ? pencils_per_warp<double>(n3[1]) : pencils_per_warp<float>(n3[1]);
+    const int lz = (zonly && !zsplit) ? 2 * n3[2] : n3[2];
+    const int pwz = c64 ? pencils_per_warp<double>(lz) : pencils_per_warp<float>(lz);
+    if (pwy <= 0 || pwz <= 0 || n3[0] % pwy || n3[0] % pwz) generic = true;
+  }
+  if (generic) {
+    for (int a = 0; a < 3; ++a)
+      if (!gen_axis_supported(n3[a]))
+        return fail(FM_ERR_UNSUPPORTED, "padded axis sizes must be at most 256, or powers of two up to 512");
+    zonly = zsplit = false;
+  }
   if (cudaSetDevice(desc->device) != cudaSuccess) return fail(FM_ERR_CUDA, "cudaSetDevice failed");
   fm_plan* P = new fm_plan();
   P->desc = *desc;
@@ -1792,6 +2000,7 @@ fm_status fm_plan_create(const fm_plan_desc* desc, fm_plan** out) {
   P->avg = avg;
   P->zonly = zonly && !zsplit;
   P->zsplit = zsplit;
+  P->generic = generic;
   for (int a = 0; a < 3; ++a) P->shift[a] = desc->absorbing[a] ? 0.25 : 0.0;
   {
     cudaDeviceProp prop;
@@ -1823,11 +2032,13 @@ void fm_plan_destroy(fm_plan* P) {
   cudaSetDevice(P->desc.device);
   if (P->st) cudaStreamSynchronize(P->st);
   DevBuf* bufs[] = {&P->twx, &P->twy, &P->twz, &P->twz2, &P->rz, &P->rxp, &P->rxm, &P->ryp, &P->rym, &P->rzp,
-                    &P->rzm, &P->V, &P->t1, &P->t2, &P->bbuf, &P->xbuf, &P->ebuf, &P->sbuf, &P->basis,
+                    &P->rzm, &P->V, &P->t1, &P->t2, &P->t3, &P->bbuf, &P->xbuf, &P->ebuf, &P->sbuf, &P->basis,
                     &P->gbuf2, &P->red_part, &P->red_out, &P->red_cnt, &P->active, &P->scale, &P->coef,
                     &P->hbuf, &P->eps_dev, &P->fx, &P->fy, &P->fz, &P->maxpart, &P->maxout, &P->wt_x,
                     &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho, &P->errbuf,
-                    &P->shifts, &P->yblk, &P->V64};
+                    &P->shifts, &P->yblk, &P->V64, &P->gtw[0], &P->gtw[1], &P->gtw[2], &P->gch[0][0],
+                    &P->gch[0][1], &P->gch[1][0], &P->gch[1][1], &P->gch[2][0], &P->gch[2][1], &P->gkn[0][0],
+                    &P->gkn[0][1], &P->gkn[1][0], &P->gkn[1][1], &P->gkn[2][0], &P->gkn[2][1]};
   for (DevBuf* b : bufs) b->release();
   tk_resolve(P);
   for (cudaEvent_t e : P->evpool) cudaEventDestroy(e);

@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(256) k_zg(Dims d, const cplx<S>* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// XI: inverse FFT along x + epilogue.
+// XI: inverse FFT along x + epilogue (g += gadd first when given).
 //   EPI_STORE    out = g
 //   EPI_OP       out = beta*out + alpha*(x - g)                 (CBSLinearOperator)
 //   EPI_PREC_OP  out = (i/eps)*V*(xs - g)                       (M^{-1} A x)
@@ -407,7 +407,35 @@ struct EpiParams {
   double inv_eps;  // 1/eps_imag (scaled units)
   const double* inv_eps_b = nullptr;  // per-RHS 1/eps_imag (null: inv_eps for all)
   const double2* shift_b = nullptr;   // EPI_PREC_OP: per-RHS shift theta, out = M^{-1}A x - theta x
+  const void* gadd = nullptr;         // storage-typed batch added to g before the epilogue (second branch of a
+                                      // two-branch average), element (x, y, z, c, b) at the contiguous batch index
 };
+
+// The epilogue on one element: g = G_avg(psi) there, ix its index within RHS b's field, vp its potential value.
+template <int EPI, typename S, typename T, typename R>
+__device__ __forceinline__ T epi_element(T g, long long ix, const cplx<S>* xvb, const cplx<S>* bvb, const cplx<S>* outb,
+                                         const cplx<S>* vp, R ie, R s, T al, T be, const EpiParams& ep, T shf) {
+  if constexpr (EPI == EPI_STORE) {
+    return g;
+  } else if constexpr (EPI == EPI_OP) {
+    T xx = cv<T>(xvb[ix]);
+    T a = cmul(al, csub(xx, g));
+    if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(outb[ix])));
+    return a;
+  } else if constexpr (EPI == EPI_PREC_OP) {
+    const T vv = cv<T>(*vp);
+    const T gam = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
+    T xx = cscale(cv<T>(xvb[ix]), s);
+    T r = cmul(gam, csub(xx, g));
+    if (ep.shift_b) r = csub(r, cmul(shf, xx));
+    return r;
+  } else {
+    const T vv = cv<T>(*vp);
+    const T gam = mk(-vv.y * ie, vv.x * ie);
+    T xx = cscale(cv<T>(xvb[ix]), s);
+    return cmul(gam, cadd(csub(cv<T>(bvb[ix]), xx), g));
+  }
+}
 
 template <typename S, typename R, int L, int EPI>
 __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 3 : 1) k_xi(Dims d, const cplx<S>* __restrict__ in, const cplx<S>* __restrict__ V,
@@ -458,26 +486,8 @@ __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 3 : 1) k_xi(Dims 
       const long long ix = rbase + x;
       T g = v[e];
       if (rampx) g = cmul(g, cconj(rampx[x]));
-      T r;
-      if constexpr (EPI == EPI_STORE) {
-        r = g;
-      } else if constexpr (EPI == EPI_OP) {
-        T xx = cv<T>(xvb[ix]);
-        T a = cmul(al, csub(xx, g));
-        if (ep.beta_re != 0.0 || ep.beta_im != 0.0) a = cadd(a, cmul(be, cv<T>(outb[ix])));
-        r = a;
-      } else if constexpr (EPI == EPI_PREC_OP) {
-        const T vv = cv<T>(Vrow[x]);
-        const T gam = mk(-vv.y * ie, vv.x * ie);  // (i/eps) * V
-        T xx = cscale(cv<T>(xvb[ix]), s);
-        r = cmul(gam, csub(xx, g));
-        if (ep.shift_b) r = csub(r, cmul(shf, xx));
-      } else {
-        const T vv = cv<T>(Vrow[x]);
-        const T gam = mk(-vv.y * ie, vv.x * ie);
-        T xx = cscale(cv<T>(xvb[ix]), s);
-        r = cmul(gam, cadd(csub(cv<T>(bvb[ix]), xx), g));
-      }
+      if (ep.gadd) g = cadd(g, cv<T>(reinterpret_cast<const cplx<S>*>(ep.gadd)[(long long)b * 3 * d.n + ix]));
+      const T r = epi_element<EPI, S, T, R>(g, ix, xvb, bvb, outb, Vrow + x, ie, s, al, be, ep, shf);
       outb[ix] = cv<TS>(r);
     }
     __syncwarp();
