@@ -396,6 +396,7 @@ def run(args):
                               "unit": "batched step"},
                 "iterations": {"min": min(iters), "max": max(iters)},
                 "born_iterations_per_s": world * sum(iters) / t_med,
+                "padded_voxel_iterations_per_s": world * sum(iters) / t_med * n_pad,
                 "flops_model": {"per_iteration": 12 * 5 * n_pad * math.log2(n_pad),
                                 "achieved_GFLOPs": world * sum(iters) / t_med * 12 * 5 * n_pad * math.log2(n_pad) / 1e9,
                                 "model": "12 x 5 N log2 N per Born iteration (2 branches x fwd+inv x 3 components)"},

@@ -1137,19 +1137,22 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
                                       (unsigned*)P->red_cnt.p, act, (int*)P->errbuf.p, P->sms, P->st));
     return e;
   }
+  auto kern = k_blockdot_mma<R, TY, S>;
+  // CTA shape: KW warps along the basis times EW along the elements, with KW * EW <= KV_WARPS and no idle warp
+  // (a basis of 9..16 groups of 8 vectors would otherwise leave up to 3 of 8 warps without work)
+  const int KG = (K + 7) / 8, GPW = S <= 4 ? 4 : 2, KW = (KG + GPW - 1) / GPW;
+  const int threads = 32 * KW * std::max(1, KV_WARPS / KW);
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockdot_mma<R, TY, S>, KV_THREADS, 0) != cudaSuccess ||
-      bps < 1)
-    bps = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, 0) != cudaSuccess || bps < 1) bps = 1;
   const long long maxb = (P->M + 127) / 128;
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   cudaError_t e = P->red_part.ensure((size_t)nb * nblk * K * S * sizeof(double2));
   if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
   if (e != cudaSuccess) return e;
   FM_TRACK(P, KC_DOT, bytes,
-           (k_blockdot_mma<R, TY, S><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, K, (const T*)U, (const TY*)Y, (double2*)P->red_part.p, (double2*)P->red_out.p,
-               (unsigned*)P->red_cnt.p, act)));
+           (kern<<<dim3(nblk, nb), threads, 0, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y,
+                                                         (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                         (unsigned*)P->red_cnt.p, act)));
   return cudaGetLastError();
 }
 
@@ -2100,20 +2103,7 @@ static fm_status apply_host(fm_plan* P, int nrhs, const double* x, double* y, in
     FM_TRY(green_op<R>(P, nrhs, P->sbuf.p, PRO_V, nullptr, EPI_OP, P->sbuf.p, nullptr, ep, P->ebuf.p, nullptr));
   } else if (mode == 2) {  // curl
     FM_TRY(h2d_field<R>(P, x, cnt, 1.0, P->sbuf.p));
-    Dims d = P->dims;
-    d.nb = nrhs;
-    FM_CK(P->t1.ensure(fbytes));
-    FM_CK(P->t2.ensure(fbytes));
-    GreenParams gp{};
-    for (int a = 0; a < 3; ++a)
-      gp.dk[a] = 2.0 * M_PI / ((double)(a == 0 ? d.nx : a == 1 ? d.ny : d.nz) * P->desc.resolution[a]);
-    gp.scale_im = -P->wavelength / (2.0 * M_PI * 377.0) / (double)P->n;
-    FM_CK(pass_xf<R>(P, d, PRO_COPY, P->sbuf.p, nullptr, nullptr, P->twx.p, nullptr, P->t1.p, nullptr));
-    FM_CK(pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
-    FM_CK(pass_zg<R>(P, d, ZMODE_CURL, P->t2.p, gp, P->twz.p, nullptr, P->t1.p, nullptr));
-    FM_CK(pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, nullptr));
-    FM_CK(pass_xi<R>(P, d, EPI_STORE, P->t2.p, nullptr, nullptr, nullptr, nullptr, ep, P->twx.p, nullptr, P->ebuf.p,
-                       nullptr));
+    FM_TRY(curl_batch<R>(P, nrhs, P->sbuf.p, P->ebuf.p, nullptr));
   }
   FM_TRY(d2h_field<R>(P, P->ebuf.p, cnt, 1.0, y));
   return check_device_error(P);

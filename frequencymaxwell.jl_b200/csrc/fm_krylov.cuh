@@ -340,8 +340,9 @@ __device__ __forceinline__ void load4(const double2* p, double2 (&v)[4]) {
   for (int q = 0; q < 4; ++q) v[q] = p[q];
 }
 
+// (not volatile: the MMA has no effect beyond its outputs, so the scheduler may move loads across it)
 __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
@@ -363,7 +364,9 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   if (active && !active[b]) return;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int gid = lane >> 2, tig = lane & 3;
-  const int KG = (K + 7) >> 3, KW = (KG + GPW - 1) / GPW, EW = KV_WARPS / KW;
+  // KW warps along the basis (GPW groups of 8 vectors each) x EW along the elements; the launcher sizes the CTA
+  // as 32 * KW * EW threads (at most KV_THREADS) so that no warp idles
+  const int KG = (K + 7) >> 3, KW = (KG + GPW - 1) / GPW, EW = (int)(blockDim.x >> 5) / KW;
   const int kw = w % KW, ew = w / KW;
   double P[GPW][NT][2], Q[GPW][NT][2];
 #pragma unroll
@@ -466,7 +469,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
 // as in k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or  Re = P0[t] - Q1[t],
 // Im = P1[t] + Q0[t]  (two tiles).
 template <typename R, typename TY, int S, typename TZ = cplx<R>>
-__global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
+__global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, TZ* Z,
                                                                 const double2* __restrict__ coef,
                                                                 const int* __restrict__ active) {
@@ -503,34 +506,44 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockupdate_mma(long long M, int
     for (int q = 0; q < 4; ++q)
 #pragma unroll
       for (int n = 0; n < NT; ++n) P[q][n][0] = P[q][n][1] = Q[q][n][0] = Q[q][n][1] = 0.0;
-    // the next 4 basis vectors are loaded before this step's MMAs: two loads in flight per lane
-    T xn[4];
+    // a ring of UPD_PD steps of basis loads (4 vectors each) stays in flight ahead of the MMAs
+    constexpr int UPD_PD = 3;
+    T xr[UPD_PD][4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      xn[q].x = 0;
-      xn[q].y = 0;
-    }
-    if (tig < K && ein) load4(ub + (size_t)tig * us + ea, xn);
-    for (int k0 = 0; k0 < K; k0 += 4) {
-      T xv[4];
+    for (int r = 0; r < UPD_PD; ++r) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        xv[q] = xn[q];
-        xn[q].x = 0;
-        xn[q].y = 0;
+        xr[r][q].x = 0;
+        xr[r][q].y = 0;
       }
-      const int kn = k0 + 4 + tig;
-      if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xn);
-      double bfr[NT];
+      const int kn = 4 * r + tig;
+      if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xr[r]);
+    }
+    for (int k0 = 0; k0 < K; k0 += 4 * UPD_PD) {
 #pragma unroll
-      for (int n = 0; n < NT; ++n) bfr[n] = Bs[k0 + tig][8 * n + gid];  // rows past K are zero
+      for (int r = 0; r < UPD_PD; ++r) {
+        const int kk = k0 + 4 * r;
+        if (kk >= K) break;  // warp-uniform
+        T xv[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const double2 x = to_d(xv[q]);
+        for (int q = 0; q < 4; ++q) {
+          xv[q] = xr[r][q];
+          xr[r][q].x = 0;
+          xr[r][q].y = 0;
+        }
+        const int kn = kk + 4 * UPD_PD + tig;
+        if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xr[r]);
+        double bfr[NT];
 #pragma unroll
-        for (int n = 0; n < NT; ++n) {
-          mma_f64(P[q][n][0], P[q][n][1], x.x, bfr[n]);
-          mma_f64(Q[q][n][0], Q[q][n][1], x.y, bfr[n]);
+        for (int n = 0; n < NT; ++n) bfr[n] = Bs[kk + tig][8 * n + gid];  // rows past K are zero
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double2 x = to_d(xv[q]);
+#pragma unroll
+          for (int n = 0; n < NT; ++n) {
+            mma_f64(P[q][n][0], P[q][n][1], x.x, bfr[n]);
+            mma_f64(Q[q][n][0], Q[q][n][1], x.y, bfr[n]);
+          }
         }
       }
     }

@@ -315,8 +315,14 @@ def run_stream(server: Server, requests: Sequence[Request], timeout: float = 360
     lat = np.array([r.latency for r in requests])
     nrhs = sum(len(r.sources) for r in requests)
     iters = sum(i["iterations"] for r in requests for i in r.infos.values())
+    # Born iterations weighted by the padded voxel count of their grid: comparable across grid shapes and with
+    # the batched solve (born_iterations_per_s x padded voxels there)
+    padded = {k: float(np.prod(e.solver.padded_size())) for k, e in server.engines.items()}
+    vox_iters = sum(i["iterations"] * padded[tuple(np.shape(r.medium.permittivity))]
+                    for r in requests for i in r.infos.values())
     return {"requests": len(requests), "solves": nrhs, "wall_s": t1 - t0, "solves_per_s": nrhs / (t1 - t0),
             "requests_per_s": len(requests) / (t1 - t0), "born_iterations_per_s": iters / (t1 - t0),
+            "padded_voxel_iterations_per_s": vox_iters / (t1 - t0),
             "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
             "offered_rate": len(requests) / max(requests[-1].arrival, 1e-9),
             "converged": sum(i["solved"] for r in requests for i in r.infos.values()),
