@@ -1157,32 +1157,53 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
 }
 
 // Z = Y - X E and the Gram matrix of Z.  TZ: type of Z (the basis type, or the block-vector type when the block
-// is stored orthonormalised afterwards and Z overwrites Y in place).
+// is stored orthonormalised afterwards and Z overwrites Y in place).  The Gram goes to red_out: the upper triangle
+// tri(t,u) for S <= 8 (k_blockgram), the full S x S matrix <Z_t, Z_u> at t*S + u for S > 8 (the block dot of Z
+// against itself on the tensor cores).
 template <typename R, typename YR, int S, typename TZ>
 static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, const void* Y, void* Z, const int* act,
                                       int nact) {
   using T = cplx<R>;
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
+  constexpr int TILE = S <= 8 ? 32 : 16;  // elements per warp tile of k_blockupdate_mma
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S, TZ>, KV_THREADS, 0) !=
           cudaSuccess ||
       bps < 1)
     bps = 1;
-  const long long maxb = (P->M + 32 * KV_WARPS - 1) / (32 * KV_WARPS);
+  const long long maxb = (P->M + TILE * KV_WARPS - 1) / (TILE * KV_WARPS);
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
            (k_blockupdate_mma<R, TY, S, TZ><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
                P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z, (const double2*)P->coef.p, act)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int nblk_g = kv_blocks(P, k_blockgram<R, S, TZ>, nb);
-  e = P->red_part.ensure((size_t)nb * nblk_g * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
-  if (e != cudaSuccess) return e;
-  FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
-           (k_blockgram<R, S, TZ><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, (const TZ*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p, act)));
-  return cudaGetLastError();
+  if constexpr (S > 8) {
+    using ZR = typename RealOf<TZ>::R;
+    auto kern = k_blockdot_mma<ZR, TZ, S>;
+    const int threads = 32 * KV_WARPS;  // K = S: two groups of 8, one warp along the basis, 8 along the elements
+    int bg = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bg, kern, threads, 0) != cudaSuccess || bg < 1) bg = 1;
+    const int nblk_g = (int)std::max(1LL, std::min<long long>((P->M + 127) / 128, (long long)P->sms * bg / nb));
+    e = P->red_part.ensure((size_t)nb * nblk_g * S * S * sizeof(double2));
+    if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(S * S, KV_KMAX + 2) * sizeof(double2));
+    if (e != cudaSuccess) return e;
+    FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
+             (kern<<<dim3(nblk_g, nb), threads, 0, P->st>>>(P->M, nb, S, (const cplx<ZR>*)Z, (const TZ*)Z,
+                                                             (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                             (unsigned*)P->red_cnt.p, act)));
+    return cudaGetLastError();
+  } else {
+    const int nblk_g = kv_blocks(P, k_blockgram<R, S, TZ>, nb);
+    e = P->red_part.ensure((size_t)nb * nblk_g * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
+    if (e != cudaSuccess) return e;
+    FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
+             (k_blockgram<R, S, TZ><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
+                 P->M, nb, (const TZ*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p,
+                 act)));
+    return cudaGetLastError();
+  }
 }
 
 // V (basis slots) = Z Rb^{-1} for the orthonormalised block storage; coefficients in P->coef
@@ -1209,7 +1230,7 @@ static cudaError_t block_kernels(fm_plan* P, int which, int S, int nb, int K, co
            : which == 2 ? launch_blockupdate<R, YR, SS, TY>(P, nb, K, U, Y, Z, act, nact)             \
                         : launch_blocknorm<R, YR, SS>(P, nb, Y, Z, act, nact);
   switch (S) {
-    FM_BLK(2) FM_BLK(3) FM_BLK(4) FM_BLK(5) FM_BLK(6) FM_BLK(7) FM_BLK(8)
+    FM_BLK(2) FM_BLK(3) FM_BLK(4) FM_BLK(5) FM_BLK(6) FM_BLK(7) FM_BLK(8) FM_BLK(16)
     default: return cudaErrorInvalidValue;
   }
 #undef FM_BLK
@@ -1235,7 +1256,7 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
   FM_CK(P->basis.ensure((size_t)cap * fbytes));
   FM_CK(P->scale.ensure((size_t)(KV_KMAX + 1) * nb * sizeof(double)));
   FM_CK(P->active.ensure((size_t)nb * sizeof(int)));
-  FM_CK(P->coef.ensure((size_t)nb * KV_KMAX * 8 * sizeof(double2)));
+  FM_CK(P->coef.ensure((size_t)nb * KV_KMAX * (std::max)(S, 8) * sizeof(double2)));
   FM_CK(P->shifts.ensure((size_t)nb * sizeof(double2)));
   FM_CK(P->yblk.ensure((size_t)(S + 1) * nb * fe * sizeof(TY)));
   FM_TRY(ensure_reduce(P, nb, KV_KMAX));
@@ -1399,18 +1420,18 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       if (acth[b]) k0 = St[b].b0[m];
     const int nc = m - k0 + 1;
     {
-      std::vector<double2> cc((size_t)nb * 8, make_double2(0, 0));
+      std::vector<double2> cc((size_t)nb * 16, make_double2(0, 0));
       for (int b = 0; b < nb; ++b) {
         if (!acth[b]) continue;
         std::vector<cd> em(K, 0.0), d(K, 0.0);
         em[m] = 1.0;
         rf_solve(St[b], K, em.data(), d.data());
-        for (int a2 = 0; a2 < nc; ++a2) cc[(size_t)b * 8 + a2] = make_double2(d[k0 + a2].real(), d[k0 + a2].imag());
+        for (int a2 = 0; a2 < nc; ++a2) cc[(size_t)b * 16 + a2] = make_double2(d[k0 + a2].real(), d[k0 + a2].imag());
       }
       FM_CK(cudaMemcpyAsync(P->coef.p, cc.data(), cc.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
       FM_TRACK(P, KC_AXPBY, (double)nc * nact * fe * sizeof(T) + (double)nact * fe * sizeof(TY),
                (k_combine<R, TY><<<dim3(2 * P->sms, nb), KV_THREADS, 0, P->st>>>(
-                   P->M, nb, k0, nc, U, (const double2*)P->coef.p, 8, Yb, act)));
+                   P->M, nb, k0, nc, U, (const double2*)P->coef.p, 16, Yb, act)));
       FM_CK(cudaGetLastError());
     }
     // Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}, t = 1..S
@@ -1457,7 +1478,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       FM_CK((block_kernels<R, YR>(P, 2, S, nb, K, U, Yb + (size_t)nb * fe, Yb + (size_t)nb * fe, act, nact)));
     else
       FM_CK((block_kernels<R, YR>(P, 1, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
-    const int NG = S * (S + 1) / 2;
+    // Gram of Y': the upper triangle tri(t,u) per RHS (S <= 8), or the full matrix at t*S + u (S > 8)
+    const int NG = S <= 8 ? S * (S + 1) / 2 : S * S;
     std::vector<double2> Gt((size_t)nb * NG);
     FM_CK(cudaMemcpyAsync(Gt.data(), P->red_out.p, Gt.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     FM_CK(cudaStreamSynchronize(P->st));
@@ -1470,7 +1492,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       int gi = 0;
       for (int t = 0; t < S; ++t)
         for (int u = t; u < S; ++u, ++gi) {
-          const cd v(Gt[(size_t)b * NG + gi].x, Gt[(size_t)b * NG + gi].y);
+          const size_t at = (size_t)b * NG + (S <= 8 ? (size_t)gi : (size_t)t * S + u);
+          const cd v(Gt[at].x, Gt[at].y);
           G[t + (size_t)u * S] = v;
           G[u + (size_t)t * S] = std::conj(v);
         }
@@ -1879,7 +1902,8 @@ static fm_status validate_opts(const fm_solve_opts* o) {
   if (o->method < 0 || o->method > 2) return fail(FM_ERR_INVALID, "unknown method");
   if (o->ortho < 0 || o->ortho > 3) return fail(FM_ERR_INVALID, "unknown orthogonalisation");
   if (o->ortho == FM_ORTHO_BLOCK && o->method == FM_METHOD_GMRES) {
-    if (o->block != 0 && (o->block < 2 || o->block > 8)) return fail(FM_ERR_INVALID, "block size must be 2..8");
+    if (o->block != 0 && (o->block < 2 || (o->block > 8 && o->block != 16)))
+      return fail(FM_ERR_INVALID, "block size must be 2..8 or 16");
     if (o->block_store != FM_BLOCK_FP64 && o->block_store != FM_BLOCK_STORAGE && o->block_store != FM_BLOCK_FP64_ORTHO)
       return fail(FM_ERR_INVALID, "unknown block vector storage");
     if (o->restart > 0) return fail(FM_ERR_UNSUPPORTED, "block GMRES runs full GMRES only (restart = 0)");
@@ -2561,6 +2585,10 @@ fm_status fm_plan_set_tuning(fm_plan* P, int knob, int value) {
       if (value != 128 && value != 256) return fail(FM_ERR_INVALID, "row-pass threads must be 128 or 256");
       P->dims.row_threads = value;
       return FM_OK;
+    case FM_TUNE_Z_SPLIT:
+      if (value < 0 || value > 2) return fail(FM_ERR_INVALID, "z-split tuning value must be 0, 1 or 2");
+      P->dims.z3 = value;
+      return FM_OK;
     case FM_TUNE_WAVE_RHS:
       if (value < 0) return fail(FM_ERR_INVALID, "right-hand sides per wave must be >= 0");
       P->wave_rhs = value;
@@ -2581,6 +2609,7 @@ fm_status fm_plan_get_tuning(fm_plan* P, int knob, int* value) {
     case FM_TUNE_Z_TMA: *value = P->tma_z ? 1 : 0; return FM_OK;
     case FM_TUNE_TMA_CTAS_PER_SM: *value = P->dims.tma_ctas; return FM_OK;
     case FM_TUNE_ROW_THREADS: *value = P->dims.row_threads; return FM_OK;
+    case FM_TUNE_Z_SPLIT: *value = P->dims.z3; return FM_OK;
     case FM_TUNE_WAVE_RHS: *value = P->wave_rhs; return FM_OK;
     case FM_TUNE_BLOCK_DOT: *value = P->bd_bulk ? 1 : 0; return FM_OK;
     default: return fail(FM_ERR_INVALID, "unknown tuning knob");

@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_combine(long long M, int B, int 
                                                         const int* __restrict__ active) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
-  __shared__ double2 cc[8];
+  __shared__ double2 cc[16];
   if (threadIdx.x < n) cc[threadIdx.x] = c[(size_t)b * cs + threadIdx.x];
   __syncthreads();
   TY* ob = out + (size_t)b * M;
@@ -347,18 +347,22 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
                : "d"(a), "d"(b));
 }
 
-// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 8)
-// S <= 4: one B tile; S > 4: two tiles (tile 0: Re Y_t, tile 1: Im Y_t, column t), so that
-//   Re = P0[t] + Q1[t],  Im = P1[t] - Q0[t]  within each lane.
+// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 16)
+// S <= 4: one B tile; S > 4: NTH = ceil(S/8) tiles of real parts then NTH tiles of imaginary parts (tile h holds
+// block vectors 8h .. 8h+7 in its columns), so that for t = 8h + c
+//   Re = P[h][c] + Q[NTH + h][c],  Im = P[NTH + h][c] - Q[h][c]  within each lane.
 template <typename R, typename TY, int S>
-__global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B, int K, const cplx<R>* __restrict__ U,
+__global__ void __launch_bounds__(KV_THREADS, S > 8 ? 2 : 1) k_blockdot_mma(long long M, int B, int K, const cplx<R>* __restrict__ U,
                                                              const TY* __restrict__ Y, double2* __restrict__ part,
                                                              double2* __restrict__ out, unsigned* __restrict__ counter,
                                                              const int* __restrict__ active) {
-  static_assert(S >= 1 && S <= 8, "block dot on tensor cores takes 1..8 block vectors");
+  static_assert(S >= 1 && S <= 16, "block dot on tensor cores takes 1..16 block vectors");
   using T = cplx<R>;
-  constexpr int NT = S <= 4 ? 1 : 2;   // 8-column B tiles
-  constexpr int GPW = S <= 4 ? 4 : 2;  // groups of 8 basis vectors per warp
+  constexpr int NTH = S <= 4 ? 1 : (S + 7) / 8;  // 8-column tiles per part
+  constexpr int NT = S <= 4 ? 1 : 2 * NTH;       // B tiles
+  constexpr int GPW = S <= 4 ? 4 : 2;            // groups of 8 basis vectors per warp
+  constexpr int HR = S <= 8 ? 2 : 1;             // runs of 4 elements per lane in a warp step
+  constexpr int WSTEP = 16 * HR;                 // elements per warp step
   __shared__ double2 red[KV_WARPS][GPW * 8][S];
   const int b = blockIdx.y, nblk = gridDim.x;
   if (active && !active[b]) return;
@@ -378,26 +382,31 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   const size_t us = (size_t)B * M;
   const T* ub = U + (size_t)b * M;
   const TY* yb = Y + (size_t)b * M;
-  const int yt = NT == 1 ? (gid & 3) : gid;  // block vector of this lane's B column
-  const bool yon = yt < S;
   if (ew < EW) {
-    // a warp step covers 32 elements: two runs of 4 per lane (h = 0, 1), i.e. twice the loads in flight
-    for (long long e0 = lo + (long long)ew * 32; e0 < hi; e0 += (long long)EW * 32) {
-      double bf[NT][2][4];
-      bool ein[2];
+    // a warp step covers WSTEP elements: HR runs of 4 per lane
+    for (long long e0 = lo + (long long)ew * WSTEP; e0 < hi; e0 += (long long)EW * WSTEP) {
+      double bf[NT][HR][4];
+      bool ein[HR];
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < HR; ++h) {
         const long long eb = e0 + 16 * h + 4 * tig;  // wholly inside or outside the range
         ein[h] = eb < hi;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          double2 y = make_double2(0.0, 0.0);
-          if (yon && ein[h]) y = to_d(yb[yt * us + eb + q]);
           if constexpr (NT == 1) {
+            const int yt = gid & 3;  // block vector of this lane's B column
+            double2 y = make_double2(0.0, 0.0);
+            if (yt < S && ein[h]) y = to_d(yb[yt * us + eb + q]);
             bf[0][h][q] = gid >= 4 ? y.y : y.x;
           } else {
-            bf[0][h][q] = y.x;
-            bf[NT - 1][h][q] = y.y;
+#pragma unroll
+            for (int th = 0; th < NTH; ++th) {
+              const int yt = 8 * th + gid;
+              double2 y = make_double2(0.0, 0.0);
+              if (yt < S && ein[h]) y = to_d(yb[yt * us + eb + q]);
+              bf[th][h][q] = y.x;
+              bf[NTH + th][h][q] = y.y;
+            }
           }
         }
       }
@@ -405,9 +414,9 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
       for (int g = 0; g < GPW; ++g) {
         if ((kw * GPW + g) >= KG) break;  // warp-uniform
         const int k = (kw * GPW + g) * 8 + gid;
-        T xv[2][4];
+        T xv[HR][4];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < HR; ++h) {
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             xv[h][q].x = 0;
@@ -416,7 +425,7 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
           if (k < K && ein[h]) load4(ub + (size_t)k * us + e0 + 16 * h + 4 * tig, xv[h]);
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < HR; ++h)
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const double2 x = to_d(xv[h][q]);
@@ -442,10 +451,14 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
       }
     } else {
 #pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int t = 2 * tig + i;
-        if (t < S) red[w][g * 8 + gid][t] = make_double2(P[g][0][i] + Q[g][NT - 1][i], P[g][NT - 1][i] - Q[g][0][i]);
-      }
+      for (int th = 0; th < NTH; ++th)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int t = 8 * th + 2 * tig + i;
+          if (t < S)
+            red[w][g * 8 + gid][t] =
+                make_double2(P[g][th][i] + Q[g][NTH + th][i], P[g][NTH + th][i] - Q[g][th][i]);
+        }
     }
   }
   __syncthreads();
@@ -464,25 +477,50 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockdot_mma(long long M, int B,
   finish_reduce(part, out, counter, KS, nblk, b);
 }
 
-// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 8).  A warp owns 32 elements
-// (lane gid: elements 4 gid .. 4 gid + 3 of the tile) and runs over the basis 4 vectors at a time.  B tiles
-// as in k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or  Re = P0[t] - Q1[t],
-// Im = P1[t] + Q0[t]  (two tiles).
+// runs of QR consecutive complex values starting at an aligned address
+template <int QR, typename C>
+__device__ __forceinline__ void load_run(const C* p, C (&v)[QR]) {
+  if constexpr (QR == 4) {
+    load4(p, v);
+  } else if constexpr (QR == 2 && sizeof(C) == 8) {
+    const float4 a = reinterpret_cast<const float4*>(p)[0];  // two complex FP32 values, 16-byte aligned
+    v[0] = make_float2(a.x, a.y);
+    v[1] = make_float2(a.z, a.w);
+  } else {
+#pragma unroll
+    for (int q = 0; q < QR; ++q) v[q] = p[q];
+  }
+}
+
+// Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 16).  A warp owns 8*QR elements (lane
+// gid: elements QR gid .. QR gid + QR - 1 of the tile) and runs over the basis 4 vectors at a time.  B tiles as in
+// k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or, for t = 8h + c,
+// Re = P[h][c] - Q[NTH + h][c],  Im = P[NTH + h][c] + Q[h][c].
 template <typename R, typename TY, int S, typename TZ = cplx<R>>
 __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, TZ* Z,
                                                                 const double2* __restrict__ coef,
                                                                 const int* __restrict__ active) {
-  static_assert(S >= 1 && S <= 8, "block update on tensor cores takes 1..8 block vectors");
+  static_assert(S >= 1 && S <= 16, "block update on tensor cores takes 1..16 block vectors");
   using T = cplx<R>;
-  constexpr int NT = S <= 4 ? 1 : 2;
+  constexpr int NTH = S <= 4 ? 1 : (S + 7) / 8;
+  constexpr int NT = S <= 4 ? 1 : 2 * NTH;
+  constexpr int QR = S <= 8 ? 4 : 2;  // elements per lane (A rows of QR MMAs)
+  constexpr int TILE = 8 * QR;        // elements per warp tile
   __shared__ double Bs[KV_KMAX][8 * NT];
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   for (int i = threadIdx.x; i < KV_KMAX * 8 * NT; i += blockDim.x) {
     const int k = i / (8 * NT), col = i - k * (8 * NT);
-    const int t = NT == 1 ? (col & 3) : (col & 7);
-    const bool im = NT == 1 ? (col >= 4) : (col >= 8);
+    int t;
+    bool im;
+    if constexpr (NT == 1) {
+      t = col & 3;
+      im = col >= 4;
+    } else {
+      im = col >= 8 * NTH;
+      t = 8 * ((col >> 3) % NTH) + (col & 7);
+    }
     double v = 0.0;
     if (k < K && t < S) {
       const double2 c = coef[(size_t)b * KV_KMAX * S + k * S + t];
@@ -497,47 +535,47 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
   const T* ub = U + (size_t)b * M;
   const TY* yb = Y + (size_t)b * M;
   TZ* zb = Z + (size_t)b * M;
-  const long long tiles = (M + 31) / 32;
+  const long long tiles = (M + TILE - 1) / TILE;
   for (long long tl = (long long)blockIdx.x * KV_WARPS + w; tl < tiles; tl += (long long)gridDim.x * KV_WARPS) {
-    const long long ea = tl * 32 + 4 * gid;  // A rows of this lane: elements ea .. ea + 3 (wholly in or out)
+    const long long ea = tl * TILE + QR * gid;  // A rows of this lane: elements ea .. ea + QR - 1 (wholly in or out)
     const bool ein = ea < M;
-    double P[4][NT][2], Q[4][NT][2];
+    double P[QR][NT][2], Q[QR][NT][2];
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < QR; ++q)
 #pragma unroll
       for (int n = 0; n < NT; ++n) P[q][n][0] = P[q][n][1] = Q[q][n][0] = Q[q][n][1] = 0.0;
     // a ring of UPD_PD steps of basis loads (4 vectors each) stays in flight ahead of the MMAs
     constexpr int UPD_PD = 3;
-    T xr[UPD_PD][4];
+    T xr[UPD_PD][QR];
 #pragma unroll
     for (int r = 0; r < UPD_PD; ++r) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < QR; ++q) {
         xr[r][q].x = 0;
         xr[r][q].y = 0;
       }
       const int kn = 4 * r + tig;
-      if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xr[r]);
+      if (kn < K && ein) load_run<QR>(ub + (size_t)kn * us + ea, xr[r]);
     }
     for (int k0 = 0; k0 < K; k0 += 4 * UPD_PD) {
 #pragma unroll
       for (int r = 0; r < UPD_PD; ++r) {
         const int kk = k0 + 4 * r;
         if (kk >= K) break;  // warp-uniform
-        T xv[4];
+        T xv[QR];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < QR; ++q) {
           xv[q] = xr[r][q];
           xr[r][q].x = 0;
           xr[r][q].y = 0;
         }
         const int kn = kk + 4 * UPD_PD + tig;
-        if (kn < K && ein) load4(ub + (size_t)kn * us + ea, xr[r]);
+        if (kn < K && ein) load_run<QR>(ub + (size_t)kn * us + ea, xr[r]);
         double bfr[NT];
 #pragma unroll
         for (int n = 0; n < NT; ++n) bfr[n] = Bs[kk + tig][8 * n + gid];  // rows past K are zero
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < QR; ++q) {
           const double2 x = to_d(xv[q]);
 #pragma unroll
           for (int n = 0; n < NT; ++n) {
@@ -547,9 +585,9 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
         }
       }
     }
-    // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1
+    // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1 of each tile
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < QR; ++q) {
       const long long e = ea + q;
       if constexpr (NT == 1) {
         const double pp0 = __shfl_xor_sync(0xffffffffu, P[q][0][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[q][0][1], 2);
@@ -567,14 +605,16 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
         }
       } else if (ein) {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int t = 2 * tig + i;
-          if (t < S) {
-            const double2 y = to_d(yb[t * us + e]);
-            zb[t * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][i] - Q[q][NT - 1][i]),
-                                                    y.y - (P[q][NT - 1][i] + Q[q][0][i])));
+        for (int th = 0; th < NTH; ++th)
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int t = 8 * th + 2 * tig + i;
+            if (t < S) {
+              const double2 y = to_d(yb[t * us + e]);
+              zb[t * us + e] = from_d<TZ>(make_double2(y.x - (P[q][th][i] - Q[q][NTH + th][i]),
+                                                      y.y - (P[q][NTH + th][i] + Q[q][th][i])));
+            }
           }
-        }
       }
     }
   }

@@ -31,7 +31,7 @@ def _solve(grid, radius, precision, block, tol=1e-6, sources=None, store="fp64")
 
 
 @pytest.mark.parametrize("precision,block", [("float64", 2), ("float64", 3), ("float64", 4), ("float64", 5),
-                                             ("float64", 6), ("float64", 8), ("float32-math64", 3),
+                                             ("float64", 6), ("float64", 8), ("float64", 16), ("float32-math64", 3),
                                              ("float32-math64", 4), ("float32-math64", 5), ("float32-math64", 6),
                                              ("float32", 4)])
 def test_block_gmres_matches_oracle(precision, block):
@@ -85,7 +85,8 @@ def test_block_gmres_oblique_fp32_math64(store):
 
 def test_block_gmres_rejects_restart_and_bad_sizes():
     grid = (16, 16, 8)
-    for ls in (F.KrylovJL_GMRES(ortho="block", gmres_restart=10), F.KrylovJL_GMRES(ortho="block", block_size=9)):
+    for ls in (F.KrylovJL_GMRES(ortho="block", gmres_restart=10), F.KrylovJL_GMRES(ortho="block", block_size=9),
+               F.KrylovJL_GMRES(ortho="block", block_size=17)):
         ocfg, solver = configs(grid, absorbing_z(8), linear_solver=ls)
         with pytest.raises((ValueError, F._lib.FMError)):
             F.solve(solver, xpol()[1], F.Medium(bead(grid, 2.0), EPS_BG))
@@ -123,8 +124,8 @@ def test_bulk_block_dot_matches_register_block_dot(precision, block):
     solver.release()
 
 
-@pytest.mark.parametrize("precision,block", [("float64", 4), ("float64", 8), ("float32-math64", 4),
-                                             ("float32-math64", 8)])
+@pytest.mark.parametrize("precision,block", [("float64", 4), ("float64", 8), ("float64", 16), ("float32-math64", 4),
+                                             ("float32-math64", 8), ("float32-math64", 16)])
 def test_block_gmres_orthonormal_block_storage(precision, block):
     """Blocks stored orthonormalised (V = Y' Rb^{-1}) take the iterates of full GMRES like raw storage."""
     ref, out, solver = _solve((32, 32, 16), 4.0, precision, block, store="fp64-ortho")
