@@ -230,9 +230,6 @@ def run(args):
     if args.block_dot >= 0:
         from fmcuda import autotune as AT
         AT.apply(solver.plan(), {"block_dot": args.block_dot})
-    if args.z_split >= 0:
-        from fmcuda import autotune as AT
-        AT.apply(solver.plan(), {"z_split": args.z_split})
     plan = solver.plan()
     info = plan.build_potential(med.permittivity, med.permittivity_bg, WL, solver.attenuation_filters(), -1)
     opts = solver.solve_options(int(info.bornmax))
@@ -560,8 +557,6 @@ def main():
     ap.add_argument("--autotune", type=int, default=1, help="1: pick launch shapes and block size with fmcuda.autotune")
     ap.add_argument("--block-dot", type=int, default=-1,
                     help="block dot of block GMRES: 1 bulk-copy pipeline, 0 register-staged, -1 the plan's default")
-    ap.add_argument("--z-split", type=int, default=-1,
-                    help="FP64 z pass: 1/2 components on three warps (24/12 warps a CTA), 0 one warp per pencil, -1 default")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--fp64-steps", type=int, default=3)

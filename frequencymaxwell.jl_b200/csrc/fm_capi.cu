@@ -1167,16 +1167,17 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
   constexpr int TILE = S <= 8 ? 32 : 16;  // elements per warp tile of k_blockupdate_mma
+  constexpr size_t ring = blockupdate_ring_bytes<R, S>();
+  auto kern = k_blockupdate_mma<R, TY, S, TZ>;
+  // the ring and the static coefficient tile together exceed the default 48 KB a block: opt in
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring);
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_blockupdate_mma<R, TY, S, TZ>, KV_THREADS, 0) !=
-          cudaSuccess ||
-      bps < 1)
-    bps = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, KV_THREADS, ring) != cudaSuccess || bps < 1) bps = 1;
   const long long maxb = (P->M + TILE * KV_WARPS - 1) / (TILE * KV_WARPS);
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
-           (k_blockupdate_mma<R, TY, S, TZ><<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z, (const double2*)P->coef.p, act)));
+           (kern<<<dim3(nblk, nb), KV_THREADS, ring, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z,
+                                                               (const double2*)P->coef.p, act)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if constexpr (S > 8) {
@@ -2585,10 +2586,6 @@ fm_status fm_plan_set_tuning(fm_plan* P, int knob, int value) {
       if (value != 128 && value != 256) return fail(FM_ERR_INVALID, "row-pass threads must be 128 or 256");
       P->dims.row_threads = value;
       return FM_OK;
-    case FM_TUNE_Z_SPLIT:
-      if (value < 0 || value > 2) return fail(FM_ERR_INVALID, "z-split tuning value must be 0, 1 or 2");
-      P->dims.z3 = value;
-      return FM_OK;
     case FM_TUNE_WAVE_RHS:
       if (value < 0) return fail(FM_ERR_INVALID, "right-hand sides per wave must be >= 0");
       P->wave_rhs = value;
@@ -2609,7 +2606,6 @@ fm_status fm_plan_get_tuning(fm_plan* P, int knob, int* value) {
     case FM_TUNE_Z_TMA: *value = P->tma_z ? 1 : 0; return FM_OK;
     case FM_TUNE_TMA_CTAS_PER_SM: *value = P->dims.tma_ctas; return FM_OK;
     case FM_TUNE_ROW_THREADS: *value = P->dims.row_threads; return FM_OK;
-    case FM_TUNE_Z_SPLIT: *value = P->dims.z3; return FM_OK;
     case FM_TUNE_WAVE_RHS: *value = P->wave_rhs; return FM_OK;
     case FM_TUNE_BLOCK_DOT: *value = P->bd_bulk ? 1 : 0; return FM_OK;
     default: return fail(FM_ERR_INVALID, "unknown tuning knob");

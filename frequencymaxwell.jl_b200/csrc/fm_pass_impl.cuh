@@ -271,20 +271,6 @@ static cudaError_t y_tma_L(const Dims& d, const void* in, const void* tw, const 
   return cudaGetLastError();
 }
 
-template <typename S, typename R, int L, int MODE, int GMAX>
-static cudaError_t zg3_launch(const Dims& d, const CUtensorMap& mi, const CUtensorMap& mo, const GreenParams& gp,
-                              const void* tw, const void* rz, const int* act, int* err, int sms, cudaStream_t st,
-                              long long ntiles) {
-  using C3 = Z3Cfg<S, R, L, MODE, GMAX>;
-  if (C3::SM::total > 227 * 1024) return cudaErrorNotSupported;
-  const size_t smem3 = C3::SM::total;
-  allow_smem(k_zg_tma3<S, R, L, MODE, GMAX>, smem3);
-  const unsigned grid3 = persistent_grid(k_zg_tma3<S, R, L, MODE, GMAX>, C3::THREADS, smem3, ntiles, sms, d.tma_ctas);
-  k_zg_tma3<S, R, L, MODE, GMAX><<<grid3, C3::THREADS, smem3, st>>>(d, mi, mo, gp, (const cplx<R>*)tw,
-                                                                    (const cplx<R>*)rz, act, err);
-  return cudaGetLastError();
-}
-
 template <typename S, typename R, int L, int MODE>
 static cudaError_t zg_tma_L(const Dims& d, const void* in, const GreenParams& gp, const void* tw, const void* rz,
                             void* out, const int* act, int* err, int sms, cudaStream_t st) {
@@ -295,17 +281,6 @@ static cudaError_t zg_tma_L(const Dims& d, const void* in, const GreenParams& gp
       !make_map(&mo, out, d, (int)sizeof(cplx<S>), 4, 1, L))
     return cudaErrorNotSupported;
   const long long ntiles = (long long)(d.nx / C::TX) * d.ny * d.nb;
-  if constexpr (std::is_same<R, double>::value) {
-    // FP64 arithmetic: the component-split kernel (three warps per pencil group), 24 (z3 = 1) or 12 (z3 = 2) warps
-    // a CTA, where its shared memory fits
-    if (d.z3 == 1) {
-      cudaError_t e = zg3_launch<S, R, L, MODE, 8>(d, mi, mo, gp, tw, rz, act, err, sms, st, ntiles);
-      if (e != cudaErrorNotSupported) return e;
-    } else if (d.z3 == 2) {
-      cudaError_t e = zg3_launch<S, R, L, MODE, 4>(d, mi, mo, gp, tw, rz, act, err, sms, st, ntiles);
-      if (e != cudaErrorNotSupported) return e;
-    }
-  }
   const size_t smem = C::SM::total;
   allow_smem(k_zg_tma<S, R, L, MODE>, smem);
   const unsigned grid = persistent_grid(k_zg_tma<S, R, L, MODE>, C::THREADS, smem, ntiles, sms, d.tma_ctas);

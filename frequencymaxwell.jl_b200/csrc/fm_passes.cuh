@@ -30,7 +30,6 @@ struct Dims {
   long long vstride = 0; // potential of RHS b at V + b*vstride (0: one potential shared by all RHS)
   int row_threads = 256; // launch shape (tuning): threads per block of the x and y row passes (128 or 256)
   int tma_ctas = 0;      // launch shape (tuning): persistent CTAs per SM of the TMA passes (0: occupancy limit)
-  int z3 = 1;            // launch shape (tuning): FP64 z pass with the components split over three warps
 };
 
 // Optional per-RHS vector pointers (RHS b's field starts at tab[b]); null -> contiguous batch.

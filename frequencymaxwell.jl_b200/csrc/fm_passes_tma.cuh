@@ -341,226 +341,4 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
   }
 }
 
-// ---------------------------------------------------------------------------
-// z pass with the components split over warps (FP64 arithmetic): three warps per pencil group, warp c transforms
-// component c.  Same arithmetic as k_zg_tma; the data path differs.  After the forward transforms each warp leaves
-// its spectrum in its own exchange buffer, the three warps of a group meet at a named barrier, each applies the
-// 3x3 product to a third of the bins (reading and writing all three spectra), meet again, and run the inverse
-// transform of their component.  A warp holds one component (E values) instead of three, so three times the warps
-// fit on an SM.
-// ---------------------------------------------------------------------------
-// GMAX: pencil groups per round at most (8: up to 24 warps a CTA; 4: up to 12 warps with more registers each).
-template <typename S, typename R, int L, int MODE, int GMAX = 8>
-struct Z3Cfg {
-  using T = cplx<R>;
-  using TS = cplx<S>;
-  static constexpr int LF = (MODE == ZMODE_AVG2) ? 2 * L : L;
-  using P = Plan<LF, R>;
-  static constexpr int TX = 128 / (int)sizeof(TS);
-  static constexpr int PW = 32 / P::TP;
-  static constexpr int NPG = TX / PW;                    // pencil groups of a tile
-  static constexpr int G3 = NPG < GMAX ? NPG : GMAX;    // groups per round (3 warps each)
-  static constexpr int ROUNDS = NPG / G3;
-  static constexpr int WARPS = 3 * G3;
-  static constexpr int THREADS = WARPS * 32;
-  static constexpr int TILE = 3 * L * 128;
-  static constexpr int STRIDE = PencilStride<LF, T, P::TP, true>::v;
-  static constexpr int EXB = WARPS * PW * STRIDE * (int)sizeof(T);
-  static constexpr int TABB = (2 * LF + L) * (int)sizeof(T);
-  // two tile stages (a load in flight while the current tile computes) when they fit beside the buffers
-  static constexpr int NST = TmaSmem<TILE, 2, EXB, TABB>::total <= 227 * 1024 ? 2 : 1;
-  using SM = TmaSmem<TILE, NST, EXB, TABB>;
-};
-
-template <typename S, typename R, int L, int MODE, int GMAX>
-__global__ void __launch_bounds__(Z3Cfg<S, R, L, MODE, GMAX>::THREADS)
-    k_zg_tma3(Dims d, const __grid_constant__ CUtensorMap tm_in, const __grid_constant__ CUtensorMap tm_out,
-              GreenParams gp, const cplx<R>* __restrict__ twz, const cplx<R>* __restrict__ rz,
-              const int* __restrict__ active, int* __restrict__ err) {
-  using C = Z3Cfg<S, R, L, MODE, GMAX>;
-  using T = typename C::T;
-  using TS = typename C::TS;
-  using P_ = typename C::P;
-  constexpr int LF = C::LF, E = P_::E, TP = P_::TP, PW = C::PW, NST = C::NST, TX = C::TX, G3 = C::G3;
-  extern __shared__ unsigned char smraw_[];
-  unsigned char* sm0 = (unsigned char*)(((uintptr_t)smraw_ + 1023) & ~(uintptr_t)1023);
-  unsigned char* tiles = sm0 + C::SM::tiles;
-  T* ex = reinterpret_cast<T*>(sm0 + C::SM::ex);
-  T* tw = reinterpret_cast<T*>(sm0 + C::SM::tab);
-  T* twr = tw + LF;
-  T* rtab = twr + LF;
-  uint64_t* full = reinterpret_cast<uint64_t*>(sm0 + C::SM::bars);
-  uint64_t* done = full + NST;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int grp = warp / 3, comp = warp - 3 * grp;  // pencil group and component of this warp
-  __shared__ int vote[C::WARPS];
-  const int xtiles = d.nx / TX;
-  const long long per_rhs = (long long)xtiles * d.ny;
-  const long long ntiles = per_rhs * d.nb;
-  load_table(tw, twz, 2 * LF);
-  if (rz) load_table(rtab, rz, L);
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < NST; ++s) {
-      mbar_init(full + s, 1);
-      mbar_init(done + s, C::WARPS);
-    }
-    fence_barrier_init();
-  }
-  __syncthreads();
-  auto issue = [&](long long tile, int s) {
-    const int xt = (int)(tile % xtiles);
-    const long long yb = tile / xtiles;
-    mbar_expect_tx(full + s, C::TILE);
-    tma_load_4d(tiles + s * C::TILE, &tm_in, full + s, xt * 16, (int)(yb % d.ny), 0, 3 * (int)(yb / d.ny));
-  };
-  long long ld = next_active(blockIdx.x, ntiles, per_rhs, active);
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < NST && ld < ntiles; ++s) {
-      issue(ld, s);
-      ld = next_active(ld + gridDim.x, ntiles, per_rhs, active);
-    }
-  }
-  const int p = lane / TP, t = lane % TP;
-  // the buffers of the three warps of this group (component c at grp*3 + c), pencil p
-  auto buf = [&](int c) -> T* { return ex + ((grp * 3 + c) * PW + p) * C::STRIDE; };
-  T* sm = buf(comp);
-  const R ksr = (R)gp.ksq_re;
-  const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
-  int it = 0;
-  bool ok = true;
-  for (long long tile = next_active(blockIdx.x, ntiles, per_rhs, active); tile < ntiles;
-       tile = next_active(tile + gridDim.x, ntiles, per_rhs, active)) {
-    const int xt = (int)(tile % xtiles);
-    const long long yb = tile / xtiles;
-    const int y = (int)(yb % d.ny), b = (int)(yb / d.ny);
-    const int s = it % NST;
-    const uint32_t ph = (it / NST) & 1;
-    // the three warps of a group agree before any of them leaves (a warp that gave up still meets its partners
-    // at the named barrier, so no partner waits for it without end)
-    const bool got = mbar_wait(full + s, ph, err, 33);
-    if (lane == 0) vote[warp] = got ? 1 : 0;
-    named_bar(1 + grp, 96);
-    if (!(vote[3 * grp] && vote[3 * grp + 1] && vote[3 * grp + 2])) {
-      ok = false;
-      break;
-    }
-    unsigned char* tl = tiles + s * C::TILE;
-    const R ksi = gp.ksq_im_b ? (R)gp.ksq_im_b[b] : (R)gp.ksq_im;
-    const R kden = ksr * ksr + ksi * ksi;
-    const T iks = mk(ksr / kden, -ksi / kden);
-#pragma unroll 1
-    for (int rd = 0; rd < C::ROUNDS; ++rd) {
-      const int xl = (rd * G3 + grp) * PW + p;
-      const int x = xt * TX + xl;
-      // forward transform of this warp's component; its spectrum stays in the warp's buffer at natural bin order
-      {
-        T v[E];
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const int z = lay_idx<LF, E, P_::R0>(t, e);
-          T a = czero<T>();
-          if (MODE != ZMODE_AVG2 || z < L) {
-            a = cv<T>(*tile_at<TS>(tl, comp * L + z, xl));
-            if (MODE != ZMODE_CURL && rz) a = cmul(a, rtab[z]);
-          }
-          v[e] = a;
-        }
-        fft_fwd_plan<-1, P_>(v, sm, tw, t);
-        __syncwarp();
-#pragma unroll
-        for (int e = 0; e < E; ++e) sm[sm_phys<T>(lay_idx<LF, E, P_::RL>(t, e))] = v[e];
-      }
-      named_bar(1 + grp, 96);
-      // per-bin 3x3 operator on bins m = comp (mod 3)
-      {
-        R kx, ky;
-        if (MODE == ZMODE_CURL) {
-          kx = (R)gp.dk[0] * kidx_curl<R>(x, d.nx);
-          ky = (R)gp.dk[1] * kidx_curl<R>(y, d.ny);
-        } else {
-          kx = (R)gp.dk[0] * (kidx_green<R>(x, d.nx) + (R)gp.shift[0]);
-          ky = (R)gp.dk[1] * (kidx_green<R>(y, d.ny) + (R)gp.shift[1]);
-        }
-        T* s0 = buf(0);
-        T* s1 = buf(1);
-        T* s2 = buf(2);
-        for (int m = comp + 3 * t; m < LF; m += 3 * TP) {
-          R kz;
-          if constexpr (MODE == ZMODE_AVG2) {
-            if ((m & 1) == 0) kz = (R)gp.dk[2] * (kidx_green<R>(m >> 1, L) + (R)gp.shift[2]);
-            else kz = (R)gp.dk[2] * (kidx_green<R>(((m + 1) >> 1) % L, L) - (R)gp.shift[2]);
-          } else if constexpr (MODE == ZMODE_ONE) {
-            kz = (R)gp.dk[2] * (kidx_green<R>(m, L) + (R)gp.shift[2]);
-          } else {
-            kz = (R)gp.dk[2] * kidx_curl<R>(m, L);
-          }
-          const int pm = sm_phys<T>(m);
-          const T e1 = s0[pm], e2 = s1[pm], e3 = s2[pm];
-          if constexpr (MODE == ZMODE_CURL) {
-            const T isc = cmul_i<1>(sc);
-            s0[pm] = cmul(csub(cscale(e3, ky), cscale(e2, kz)), isc);
-            s1[pm] = cmul(csub(cscale(e1, kz), cscale(e3, kx)), isc);
-            s2[pm] = cmul(csub(cscale(e2, kx), cscale(e1, ky)), isc);
-          } else {
-            T kE = cmul(cadd(cadd(cscale(e1, kx), cscale(e2, ky)), cscale(e3, kz)), iks);
-            const R k2 = kx * kx + ky * ky + kz * kz;
-            const R dr = k2 - ksr, di = -ksi;
-            const R dd = dr * dr + di * di;
-            const R rdd = R(1) / dd;  // one division for both parts of 1 / (k^2 - ks)
-            const T f = cmul(sc, mk(dr * rdd, -di * rdd));
-            s0[pm] = cmul(csub(e1, cscale(kE, kx)), f);
-            s1[pm] = cmul(csub(e2, cscale(kE, ky)), f);
-            s2[pm] = cmul(csub(e3, cscale(kE, kz)), f);
-          }
-        }
-      }
-      named_bar(1 + grp, 96);
-      // inverse transform of this warp's component back into the tile
-      {
-        T v[E];
-#pragma unroll
-        for (int e = 0; e < E; ++e) v[e] = sm[sm_phys<T>(lay_idx<LF, E, P_::RL>(t, e))];
-        __syncwarp();
-        fft_rev_plan<+1, P_>(v, sm, twr, t);
-        __syncwarp();
-#pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const int z = lay_idx<LF, E, P_::R0>(t, e);
-          if (MODE != ZMODE_AVG2 || z < L) {
-            T a = v[e];
-            if (MODE != ZMODE_CURL && rz) a = cmul(a, cconj(rtab[z]));
-            *tile_at<TS>(tl, comp * L + z, xl) = cv<TS>(a);
-          }
-        }
-      }
-      __syncwarp();
-    }
-    fence_proxy_async();
-    __syncwarp();
-    if (lane == 0) mbar_arrive(done + s);
-    if (threadIdx.x == 0 && ok) {
-      // on a timeout thread 0 stops storing and loading but stays in the loop: the other warps then time out on
-      // the next load (bounded), vote, and leave together
-      if (!mbar_wait(done + s, ph, err, 34)) {
-        ok = false;
-      } else {
-        tma_store_4d(&tm_out, tl, xt * 16, y, 0, 3 * b);
-        bulk_commit();
-        bulk_wait_read0();
-        if (ld < ntiles) {
-          issue(ld, s);
-          ld = next_active(ld + gridDim.x, ntiles, per_rhs, active);
-        }
-      }
-    }
-    ++it;
-  }
-  if (threadIdx.x == 0) {
-    if (!ok) {
-      for (int k = 0; k < NST; ++k) mbar_wait(full + ((it + k) % NST), ((it + k) / NST) & 1, err, 35);
-    }
-    bulk_wait0();
-  }
-}
-
 }  // namespace fm

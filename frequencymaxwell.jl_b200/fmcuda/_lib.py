@@ -21,7 +21,6 @@ FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2, FM_ORTHO_BLOCK = 0, 1, 2, 3
 FM_BLOCK_FP64, FM_BLOCK_STORAGE, FM_BLOCK_FP64_ORTHO = 0, 1, 2
 FM_TUNE_Y_TMA, FM_TUNE_Z_TMA, FM_TUNE_TMA_CTAS_PER_SM, FM_TUNE_ROW_THREADS, FM_TUNE_WAVE_RHS = 0, 1, 2, 3, 4
 FM_TUNE_BLOCK_DOT = 5
-FM_TUNE_Z_SPLIT = 6
 
 STATUS_NAMES = {
     FM_OK: "FM_OK", FM_ERR_INVALID: "FM_ERR_INVALID", FM_ERR_OOM: "FM_ERR_OOM",

@@ -8,7 +8,6 @@ GMRES changes the order of the Gram-Schmidt arithmetic, and every candidate keep
 * ``row_threads``        -- threads per block of the x and y row passes (128 or 256)
 * ``wave_rhs``           -- right-hand sides per wave (0 = as many as device memory holds)
 * ``block_dot``          -- block dot of block GMRES: bulk-copy pipeline (1) or register-staged kernel (0)
-* ``z_split``            -- FP64 z pass with the components on three warps (1: 24 warps a CTA, 2: 12) or not (0)
 * ``block``              -- vectors per block of block GMRES (8 or 4)
 
 ``autotune`` times short fixed-work solves of the caller's own batch (tolerance 0, a few iterations) on the
@@ -28,15 +27,12 @@ from typing import Callable, Dict, List, Optional, Sequence
 
 from . import _lib as L
 
-DEFAULT = {"tma_y": 1, "tma_z": 1, "tma_ctas": 0, "row_threads": 256, "wave_rhs": 0, "block_dot": 0, "z_split": 1,
-           "block": 8}
+DEFAULT = {"tma_y": 1, "tma_z": 1, "tma_ctas": 0, "row_threads": 256, "wave_rhs": 0, "block_dot": 0, "block": 8}
 # block_dot is not searched: the trials run a few iterations (a basis of a few vectors) and did not separate the
 # two kernels, while over a full solve of 100 iterations the register-staged one is faster
-SPACE = {"tma_y": (1, 0), "tma_z": (1, 0), "tma_ctas": (0, 1, 2), "row_threads": (256, 128), "z_split": (1, 2, 0),
-         "block": (8, 4)}
+SPACE = {"tma_y": (1, 0), "tma_z": (1, 0), "tma_ctas": (0, 1, 2), "row_threads": (256, 128), "block": (8, 4)}
 _KNOB = {"tma_y": L.FM_TUNE_Y_TMA, "tma_z": L.FM_TUNE_Z_TMA, "tma_ctas": L.FM_TUNE_TMA_CTAS_PER_SM,
-         "row_threads": L.FM_TUNE_ROW_THREADS, "wave_rhs": L.FM_TUNE_WAVE_RHS, "block_dot": L.FM_TUNE_BLOCK_DOT,
-         "z_split": L.FM_TUNE_Z_SPLIT}
+         "row_threads": L.FM_TUNE_ROW_THREADS, "wave_rhs": L.FM_TUNE_WAVE_RHS, "block_dot": L.FM_TUNE_BLOCK_DOT}
 _memory: Dict[str, dict] = {}
 _lock = threading.Lock()
 

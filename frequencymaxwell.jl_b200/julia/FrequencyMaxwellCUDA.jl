@@ -36,7 +36,6 @@ const FM_TUNE_TMA_CTAS_PER_SM = Cint(2)
 const FM_TUNE_ROW_THREADS = Cint(3)
 const FM_TUNE_WAVE_RHS = Cint(4)
 const FM_TUNE_BLOCK_DOT = Cint(5)
-const FM_TUNE_Z_SPLIT = Cint(6)
 
 struct FMPlanDesc
     grid::NTuple{3,Cint}

@@ -27,7 +27,7 @@ def test_launch_knobs_do_not_change_the_operator(precision):
     ref = plan.apply_operator(x)
     tol = 1e-13 if precision == "float64" else 1e-7
     for cfg in ({"tma_y": 0}, {"tma_z": 0}, {"tma_ctas": 1}, {"row_threads": 128}, {"tma_y": 0, "tma_z": 0},
-                {"tma_ctas": 2, "row_threads": 128}, {"z_split": 0}, {"z_split": 2}, {"z_split": 2, "tma_ctas": 1}):
+                {"tma_ctas": 2, "row_threads": 128}):
         AT.apply(plan, dict(AT.DEFAULT, **cfg))
         assert AT.read(plan) == {k: v for k, v in dict(AT.DEFAULT, **cfg).items() if k != "block"}
         assert rel(plan.apply_operator(x), ref) < tol
@@ -41,7 +41,7 @@ def test_invalid_tuning_values_rejected():
     plan = solver.plan()
     lib = _lib.lib()
     for knob, value in ((_lib.FM_TUNE_Y_TMA, 2), (_lib.FM_TUNE_ROW_THREADS, 512), (_lib.FM_TUNE_TMA_CTAS_PER_SM, -1),
-                        (_lib.FM_TUNE_WAVE_RHS, -3), (_lib.FM_TUNE_BLOCK_DOT, 2), (_lib.FM_TUNE_Z_SPLIT, 3), (99, 0)):
+                        (_lib.FM_TUNE_WAVE_RHS, -3), (_lib.FM_TUNE_BLOCK_DOT, 2), (99, 0)):
         assert lib.fm_plan_set_tuning(plan.handle, knob, value) == _lib.FM_ERR_INVALID
     v = ctypes.c_int(-1)
     assert lib.fm_plan_get_tuning(plan.handle, _lib.FM_TUNE_ROW_THREADS, ctypes.byref(v)) == _lib.FM_OK
