@@ -14,7 +14,7 @@
 namespace fm {
 
 // max |k^2 (eps/eps_bg - 1)| over the unpadded grid (deterministic two-level)
-__global__ void __launch_bounds__(256) k_potential_max(long long n, const double2* __restrict__ eps, double eps_bg,
+static __global__ void __launch_bounds__(256) k_potential_max(long long n, const double2* __restrict__ eps, double eps_bg,
                                                         double k2, double* __restrict__ part, double* __restrict__ out,
                                                         unsigned* __restrict__ counter) {
   __shared__ double red[8];
