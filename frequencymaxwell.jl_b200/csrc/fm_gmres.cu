@@ -581,17 +581,14 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
   constexpr int TILE = S <= 8 ? 32 : 16;  // elements per warp tile of k_blockupdate_mma
-  constexpr size_t ring = blockupdate_ring_bytes<R, S>();
   auto kern = k_blockupdate_mma<R, TY, S, TZ>;
-  // the ring and the static coefficient tile together exceed the default 48 KB a block: opt in
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ring);
   int bps = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, KV_THREADS, ring) != cudaSuccess || bps < 1) bps = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, KV_THREADS, 0) != cudaSuccess || bps < 1) bps = 1;
   const long long maxb = (P->M + TILE * KV_WARPS - 1) / (TILE * KV_WARPS);
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
-           (kern<<<dim3(nblk, nb), KV_THREADS, ring, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z,
-                                                               (const double2*)P->coef.p, act)));
+           (kern<<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z,
+                                                            (const double2*)P->coef.p, act)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if constexpr (S > 8) {

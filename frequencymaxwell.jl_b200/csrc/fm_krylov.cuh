@@ -496,32 +496,6 @@ __device__ __forceinline__ void load_run(const C* p, C (&v)[QR]) {
 // gid: elements QR gid .. QR gid + QR - 1 of the tile) and runs over the basis 4 vectors at a time.  B tiles as in
 // k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or, for t = 8h + c,
 // Re = P[h][c] - Q[NTH + h][c],  Im = P[NTH + h][c] + Q[h][c].
-// cp.async of one lane's run of QR complex values (16-byte pieces; zero-filled when `on` is false)
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool on) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src), "r"(on ? 16 : 0)
-               : "memory");
-}
-template <int QR, typename C>
-__device__ __forceinline__ void cp_async_run(C* dst, const C* src, bool on) {
-  constexpr int pieces = QR * (int)sizeof(C) / 16;
-  static_assert(pieces >= 1 && QR * sizeof(C) % 16 == 0, "runs are whole 16-byte pieces");
-#pragma unroll
-  for (int i = 0; i < pieces; ++i)
-    cp_async16(reinterpret_cast<char*>(dst) + 16 * i, reinterpret_cast<const char*>(src) + 16 * i, on);
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-constexpr int UPD_D = 6;  // steps of basis loads in flight per lane in the block update
-
-// shared-memory bytes of k_blockupdate_mma beyond its static arrays: the per-lane ring
-template <typename R, int S>
-constexpr size_t blockupdate_ring_bytes() {
-  return (size_t)KV_THREADS * UPD_D * (S <= 8 ? 4 : 2) * sizeof(cplx<R>);
-}
-
 template <typename R, typename TY, int S, typename TZ = cplx<R>>
 __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, TZ* Z,
@@ -534,8 +508,6 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
   constexpr int QR = S <= 8 ? 4 : 2;  // elements per lane (A rows of QR MMAs)
   constexpr int TILE = 8 * QR;        // elements per warp tile
   __shared__ double Bs[KV_KMAX][8 * NT];
-  extern __shared__ __align__(16) unsigned char upd_dyn[];
-  T* upd_ring = reinterpret_cast<T*>(upd_dyn);
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   for (int i = threadIdx.x; i < KV_KMAX * 8 * NT; i += blockDim.x) {
@@ -572,42 +544,47 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
     for (int q = 0; q < QR; ++q)
 #pragma unroll
       for (int n = 0; n < NT; ++n) P[q][n][0] = P[q][n][1] = Q[q][n][0] = Q[q][n][1] = 0.0;
-    // The basis loads of UPD_D steps (4 vectors each) stay in flight ahead of the MMAs: each lane copies its own
-    // run of QR values per step into its slot of a shared-memory ring with cp.async (no registers held), waits for
-    // the oldest group, and reads back only what it copied itself.
-    T* ring = upd_ring + (size_t)(w * 32 + lane) * UPD_D * QR;
-    const int nsteps = (K + 3) / 4;
+    // a ring of UPD_PD steps of basis loads (4 vectors each) stays in flight ahead of the MMAs
+    constexpr int UPD_PD = 3;
+    T xr[UPD_PD][QR];
 #pragma unroll
-    for (int r = 0; r < UPD_D; ++r) {
-      const int kn = 4 * r + tig;
-      cp_async_run<QR>(ring + r * QR, ub + (size_t)(kn < K ? kn : 0) * us + (ein ? ea : 0), kn < K && ein);
-      cp_async_commit();
-    }
-    for (int j = 0; j < nsteps; ++j) {
-      const int kk = 4 * j;
-      cp_async_wait<UPD_D - 1>();
-      const int slot = j % UPD_D;
-      T xv[QR];
-#pragma unroll
-      for (int q = 0; q < QR; ++q) xv[q] = ring[slot * QR + q];
-      double bfr[NT];
-#pragma unroll
-      for (int n = 0; n < NT; ++n) bfr[n] = Bs[kk + tig][8 * n + gid];  // rows past K are zero
+    for (int r = 0; r < UPD_PD; ++r) {
 #pragma unroll
       for (int q = 0; q < QR; ++q) {
-        const double2 x = to_d(xv[q]);
+        xr[r][q].x = 0;
+        xr[r][q].y = 0;
+      }
+      const int kn = 4 * r + tig;
+      if (kn < K && ein) load_run<QR>(ub + (size_t)kn * us + ea, xr[r]);
+    }
+    for (int k0 = 0; k0 < K; k0 += 4 * UPD_PD) {
 #pragma unroll
-        for (int n = 0; n < NT; ++n) {
-          mma_f64(P[q][n][0], P[q][n][1], x.x, bfr[n]);
-          mma_f64(Q[q][n][0], Q[q][n][1], x.y, bfr[n]);
+      for (int r = 0; r < UPD_PD; ++r) {
+        const int kk = k0 + 4 * r;
+        if (kk >= K) break;  // warp-uniform
+        T xv[QR];
+#pragma unroll
+        for (int q = 0; q < QR; ++q) {
+          xv[q] = xr[r][q];
+          xr[r][q].x = 0;
+          xr[r][q].y = 0;
+        }
+        const int kn = kk + 4 * UPD_PD + tig;
+        if (kn < K && ein) load_run<QR>(ub + (size_t)kn * us + ea, xr[r]);
+        double bfr[NT];
+#pragma unroll
+        for (int n = 0; n < NT; ++n) bfr[n] = Bs[kk + tig][8 * n + gid];  // rows past K are zero
+#pragma unroll
+        for (int q = 0; q < QR; ++q) {
+          const double2 x = to_d(xv[q]);
+#pragma unroll
+          for (int n = 0; n < NT; ++n) {
+            mma_f64(P[q][n][0], P[q][n][1], x.x, bfr[n]);
+            mma_f64(Q[q][n][0], Q[q][n][1], x.y, bfr[n]);
+          }
         }
       }
-      // refill the slot just read (its values are in registers) with step j + UPD_D
-      const int kn = kk + 4 * UPD_D + tig;
-      cp_async_run<QR>(ring + slot * QR, ub + (size_t)(kn < K ? kn : 0) * us + (ein ? ea : 0), kn < K && ein);
-      cp_async_commit();
     }
-    cp_async_wait<0>();
     // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1 of each tile
 #pragma unroll
     for (int q = 0; q < QR; ++q) {
