@@ -734,8 +734,9 @@ fm_status fm_plan_set_tuning(fm_plan* P, int knob, int value) {
       P->wave_rhs = value;
       return FM_OK;
     case FM_TUNE_BLOCK_DOT:
-      if (value != 0 && value != 1) return fail(FM_ERR_INVALID, "block-dot tuning value must be 0 or 1");
-      P->bd_bulk = value != 0;
+      if (value < 0 || value > 2) return fail(FM_ERR_INVALID, "block-dot tuning value must be 0, 1 or 2");
+      P->bd_bulk = value == 1;
+      P->bd_wide = value == 2;
       return FM_OK;
     default:
       return fail(FM_ERR_INVALID, "unknown tuning knob");
@@ -750,7 +751,7 @@ fm_status fm_plan_get_tuning(fm_plan* P, int knob, int* value) {
     case FM_TUNE_TMA_CTAS_PER_SM: *value = P->dims.tma_ctas; return FM_OK;
     case FM_TUNE_ROW_THREADS: *value = P->dims.row_threads; return FM_OK;
     case FM_TUNE_WAVE_RHS: *value = P->wave_rhs; return FM_OK;
-    case FM_TUNE_BLOCK_DOT: *value = P->bd_bulk ? 1 : 0; return FM_OK;
+    case FM_TUNE_BLOCK_DOT: *value = P->bd_bulk ? 1 : P->bd_wide ? 2 : 0; return FM_OK;
     default: return fail(FM_ERR_INVALID, "unknown tuning knob");
   }
 }

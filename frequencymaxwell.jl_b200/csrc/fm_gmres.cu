@@ -551,10 +551,12 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
                                       (unsigned*)P->red_cnt.p, act, (int*)P->errbuf.p, P->sms, P->st));
     return e;
   }
-  auto kern = k_blockdot_mma<R, TY, S>;
+  // register kernel: two groups of 8 basis vectors per warp (tuning 0) or four (tuning 2, 5 <= S <= 8)
+  const bool wide = P->bd_wide && S > 4 && S <= 8;
+  auto kern = wide ? k_blockdot_mma<R, TY, S, (S > 4 && S <= 8)> : k_blockdot_mma<R, TY, S, false>;
   // CTA shape: KW warps along the basis times EW along the elements, with KW * EW <= KV_WARPS and no idle warp
   // (a basis of 9..16 groups of 8 vectors would otherwise leave up to 3 of 8 warps without work)
-  const int KG = (K + 7) / 8, GPW = S <= 4 ? 4 : 2, KW = (KG + GPW - 1) / GPW;
+  const int KG = (K + 7) / 8, GPW = (S <= 4 || wide) ? 4 : 2, KW = (KG + GPW - 1) / GPW;
   const int threads = 32 * KW * std::max(1, KV_WARPS / KW);
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, 0) != cudaSuccess || bps < 1) bps = 1;

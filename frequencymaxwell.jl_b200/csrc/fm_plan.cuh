@@ -85,6 +85,7 @@ struct fm_plan {
   bool use_tma = true;  // TMA-staged y/z passes (FMCUDA_NO_TMA=1 selects the register-only passes)
   bool tma_y = true, tma_z = true;  // tuning: TMA-staged y / z passes where the size has one
   bool bd_bulk = false;             // tuning: bulk-copy pipelined block dot where the shape has one
+  bool bd_wide = false;             // tuning: register block dot with four basis groups per warp (5 <= s <= 8)
   int wave_rhs = 0;                 // tuning: right-hand sides per wave at most (0: as many as memory holds)
   DevBuf errbuf;        // device error code written by bounded pipeline waits
   bool avg = false;     // any absorbing axis

@@ -241,8 +241,9 @@ void* fm_stream(fm_plan* plan);
  *   FM_TUNE_TMA_CTAS_PER_SM         persistent CTAs per SM of the TMA passes, 0 = occupancy limit
  *   FM_TUNE_ROW_THREADS             threads per block of the x and y row passes: 128 or 256
  *   FM_TUNE_WAVE_RHS                right-hand sides per wave at most, 0 = as many as device memory holds
- *   FM_TUNE_BLOCK_DOT               block dot of block GMRES: 1 = bulk-copy pipeline (one CTA per SM), 0 = the
- *                                   register-staged kernel */
+ *   FM_TUNE_BLOCK_DOT               block dot of block GMRES: 0 = the register-staged kernel, 1 = bulk-copy
+ *                                   pipeline (one CTA per SM), 2 = the register-staged kernel with four groups of
+ *                                   basis vectors per warp (blocks of 5..8 vectors) */
 enum { FM_TUNE_Y_TMA = 0, FM_TUNE_Z_TMA = 1, FM_TUNE_TMA_CTAS_PER_SM = 2, FM_TUNE_ROW_THREADS = 3,
        FM_TUNE_WAVE_RHS = 4, FM_TUNE_BLOCK_DOT = 5 };
 fm_status fm_plan_set_tuning(fm_plan* plan, int knob, int value);

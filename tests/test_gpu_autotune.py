@@ -41,7 +41,7 @@ def test_invalid_tuning_values_rejected():
     plan = solver.plan()
     lib = _lib.lib()
     for knob, value in ((_lib.FM_TUNE_Y_TMA, 2), (_lib.FM_TUNE_ROW_THREADS, 512), (_lib.FM_TUNE_TMA_CTAS_PER_SM, -1),
-                        (_lib.FM_TUNE_WAVE_RHS, -3), (_lib.FM_TUNE_BLOCK_DOT, 2), (99, 0)):
+                        (_lib.FM_TUNE_WAVE_RHS, -3), (_lib.FM_TUNE_BLOCK_DOT, 3), (99, 0)):
         assert lib.fm_plan_set_tuning(plan.handle, knob, value) == _lib.FM_ERR_INVALID
     v = ctypes.c_int(-1)
     assert lib.fm_plan_get_tuning(plan.handle, _lib.FM_TUNE_ROW_THREADS, ctypes.byref(v)) == _lib.FM_OK
