@@ -364,6 +364,9 @@ def run(args):
     serving = None
     if rank == 0 and world == 1 and args.serving_requests > 0:
         serving = run_serving(args)
+    large = None
+    if rank == 0 and world == 1 and args.large:
+        large = run_large(args)
     cb = None
     oracle_acc = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -411,7 +414,7 @@ def run(args):
                         "d2h_bytes_per_step": d2h},
                 "roofline": roof, "kernel_classes": classes,
                 "algorithmic_GBps_all_kernels": all_bytes / (total_ms / 1000) / 1e9 if total_ms else None,
-                "serving": serving, "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
+                "serving": serving, "large": large, "cpu_baseline": cb, "clocks": clocks, "gpu_launches": launches}
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -558,7 +561,7 @@ def main():
     ap.add_argument("--block-dot", type=int, default=-1,
                     help="block dot of block GMRES: 1 bulk-copy pipeline, 0 register-staged, -1 the plan's default")
     ap.add_argument("--precision", default="float32-math64", choices=["float32", "float32-math64"])
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--fp64-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--operator-case", action="store_true", help="profiling case: operator applications only")
@@ -569,7 +572,8 @@ def main():
     ap.add_argument("--serving-basis", type=int, default=100)
     ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
     ap.add_argument("--large-only", action="store_true", help="run the large single configuration and print it")
-    ap.add_argument("--large-check", type=int, default=1, help="with --large-only: FP32 vs FP64 check at 128x128x256")
+    ap.add_argument("--large-check", type=int, default=1, help="with the large configuration: FP32 vs FP64 check at 128x128x256")
+    ap.add_argument("--large", type=int, default=1, help="1: also run the large single configuration (N = 1 only)")
     args = ap.parse_args()
     if args.operator_case:
         return run_operator_case(args)
