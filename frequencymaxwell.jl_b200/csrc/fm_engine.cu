@@ -1,5 +1,6 @@
 // libfmcuda: the slot engine behind the serving loop (continuous batching of independent right-hand sides).
 #include "fm_plan.cuh"
+#include "fm_blockalg.h"
 
 // ===========================================================================
 // Slot engine: continuous batching of independent right-hand sides.
@@ -21,6 +22,14 @@
 // restart = basis (full GMRES when its iteration limit fits the basis), so its
 // result does not depend on the other slots.  All requests of an engine share
 // wavelength and background permittivity.
+//
+// With FM_ORTHO_BLOCK a slot whose iteration limit fits the basis (maxiters +
+// s + 1 stored vectors) runs the batched s-step block GMRES instead (s = 8, FP64
+// block vectors stored orthonormalised): its first s iterations share step 3's
+// CGS launches, after which each engine step advances it by one block of s
+// iterations (3b), in launches shared by every slot in that phase, each at its
+// own basis size.  The per-RHS algebra is that of the batched block solve
+// (fm_blockalg.cu).  Slots whose limit does not fit run CGS GMRES(basis).
 // ===========================================================================
 struct EngineUnit {  // one queued right-hand side
   long long req;
@@ -38,6 +47,10 @@ enum { SL_FREE = 0, SL_RUN = 1, SL_STOP = 2, SL_RESTART = 3, SL_RESIDUAL = 4 };
 struct EngineSlot {
   int state = SL_FREE;
   bool fresh = false;  // admitted, residual not formed yet
+  bool blk = false;    // s-step block GMRES (FM_ORTHO_BLOCK engines, limit fits the basis)
+  int phase = 0;       // block slots: 1 = the first s CGS steps, 2 = blocks
+  int m = 0;           // block slots: Hessenberg columns done
+  BlkState bst;
   EngineUnit u;
   int j = 0, inner = 0, iters = 0, maxiters = 100;
   double beta = 0, eps = 0, rnorm = 0, eps_imag = 0, beta0 = 0;
@@ -52,8 +65,10 @@ struct fm_engine {
   int S = 0, mem = 100;
   double wavelength = 0, eps_bg = 0;
   int ortho = FM_ORTHO_CGS;
+  int bs = 0;  // FM_ORTHO_BLOCK: vectors per block
   DevBuf U, X, Bv, Sb, Hb, Vs, ksq, ieps, scale, act, kb, tabs, Eo, Ho, wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first,
       epsd, maxp, maxo;
+  DevBuf Yb, V64s, k0d, ncd, vrowd, kbd;  // block slots: FP64 block vectors, FP64 potentials, per-slot indices
   std::vector<EngineSlot> slots;
   std::deque<EngineUnit> queue;
   std::mutex mu;
@@ -78,19 +93,34 @@ long long fm_engine_slot_bytes(const fm_plan_desc* d, int basis) {
   return 3 * n * esz * (basis + 1 + 6) + n * esz + 2 * 3 * g * 16;
 }
 
+// vectors per block of the engine's block GMRES
+static constexpr int kEngineBlock = 8;
+
+long long fm_engine_slot_bytes_ortho(const fm_plan_desc* d, int basis, int ortho) {
+  const long long base = fm_engine_slot_bytes(d, basis);
+  if (base < 0 || ortho != FM_ORTHO_BLOCK) return base;
+  long long n = 1;
+  for (int a = 0; a < 3; ++a) n *= (long long)(d->grid[a] + 2 * d->pad[a]);
+  const long long esz = d->precision == FM_PREC_F64 ? 16 : 8, ysz = d->precision == FM_PREC_F32 ? 8 : 16;
+  // block vectors Y_0..Y_s, the pass temporaries at the block-vector type, a potential of that type
+  return base + 3 * n * ysz * (kEngineBlock + 1) + 2 * 3 * n * (ysz - esz) + (ysz != esz ? n * ysz : 0);
+}
+
 fm_status fm_engine_create(fm_plan* P, int slots, int basis, double wavelength, double eps_bg, const double* fx,
                            const double* fy, const double* fz, int ortho, fm_engine** out) {
   if (!P || !out || slots < 1 || basis < 1) return fail(FM_ERR_INVALID, "fm_engine_create: bad argument");
   *out = nullptr;
   if (basis + 1 > KV_KMAX) return fail(FM_ERR_UNSUPPORTED, "Krylov basis larger than 127 vectors");
   if (!(wavelength > 0) || !(eps_bg > 0)) return fail(FM_ERR_INVALID, "wavelength and permittivity_bg must be positive");
-  if (ortho != FM_ORTHO_CGS && ortho != FM_ORTHO_CGS2) return fail(FM_ERR_INVALID, "the engine runs CGS or CGS2");
+  if (ortho != FM_ORTHO_CGS && ortho != FM_ORTHO_CGS2 && ortho != FM_ORTHO_BLOCK)
+    return fail(FM_ERR_INVALID, "the engine runs CGS, CGS2 or block GMRES");
   FM_CK(cudaSetDevice(P->desc.device));
   fm_engine* E = new fm_engine();
   E->P = P;
   E->S = slots;
   E->mem = basis;
   E->ortho = ortho;
+  E->bs = ortho == FM_ORTHO_BLOCK ? kEngineBlock : 0;
   E->wavelength = wavelength;
   E->eps_bg = eps_bg;
   const int n3[3] = {P->dims.nx, P->dims.ny, P->dims.nz};
@@ -139,10 +169,23 @@ fm_status fm_engine_create(fm_plan* P, int slots, int basis, double wavelength, 
   al(E->epsd, (size_t)g * sizeof(double2));
   al(E->maxp, 592 * sizeof(double));
   al(E->maxo, 64);
-  if (e == cudaSuccess) e = P->t1.ensure(S * M * esz);
-  if (e == cudaSuccess) e = P->t2.ensure(S * M * esz);
+  // block slots: block vectors, pass temporaries and potentials of the block-vector type (FP64 unless the plan
+  // computes in FP32), per-slot index arrays, update coefficients of a whole block
+  const size_t ysz = P->prec == FM_PREC_F32 ? esz : sizeof(double2), tsz = E->bs ? std::max(esz, ysz) : esz;
+  if (E->bs) {
+    al(E->Yb, (size_t)(E->bs + 1) * S * M * ysz);
+    if (ysz != esz) al(E->V64s, S * n * ysz);
+    al(E->k0d, S * sizeof(int));
+    al(E->ncd, S * sizeof(int));
+    al(E->vrowd, S * sizeof(int));
+    al(E->kbd, S * sizeof(int));
+    if (e == cudaSuccess) e = P->shifts.ensure(S * sizeof(double2));
+  }
+  if (e == cudaSuccess) e = P->t1.ensure(S * M * tsz);
+  if (e == cudaSuccess) e = P->t2.ensure(S * M * tsz);
   if (e == cudaSuccess) e = P->scale.ensure((size_t)(KV_KMAX + 1) * S * sizeof(double));
-  if (e == cudaSuccess) e = P->coef.ensure((size_t)(KV_KMAX + 1) * S * sizeof(double2));
+  if (e == cudaSuccess)
+    e = P->coef.ensure((size_t)(KV_KMAX + 1) * S * std::max(E->bs, 1) * sizeof(double2));
   std::vector<int> first(S + 1);
   for (size_t s = 0; s <= S; ++s) first[s] = (int)s;
   std::vector<double> zero(S, 0.0);
@@ -170,9 +213,10 @@ void fm_engine_destroy(fm_engine* E) {
   if (!E) return;
   cudaSetDevice(E->P->desc.device);
   cudaStreamSynchronize(E->P->st);
-  DevBuf* b[] = {&E->U, &E->X, &E->Bv, &E->Sb, &E->Hb, &E->Vs, &E->ksq, &E->ieps, &E->scale, &E->act, &E->kb,
-                 &E->tabs, &E->Eo, &E->Ho, &E->wt_x, &E->wt_y, &E->wt_z, &E->wt_pe, &E->wt_ph, &E->wt_first,
-                 &E->epsd, &E->maxp, &E->maxo};
+  DevBuf* b[] = {&E->U,    &E->X,    &E->Bv,    &E->Sb,       &E->Hb,   &E->Vs,   &E->ksq,  &E->ieps,
+                 &E->scale, &E->act,  &E->kb,    &E->tabs,     &E->Eo,   &E->Ho,   &E->wt_x, &E->wt_y,
+                 &E->wt_z,  &E->wt_pe, &E->wt_ph, &E->wt_first, &E->epsd, &E->maxp, &E->maxo, &E->Yb,
+                 &E->V64s,  &E->k0d,  &E->ncd,   &E->vrowd,    &E->kbd};
   for (DevBuf* x : b) x->release();
   delete E;
 }
@@ -233,9 +277,109 @@ static int engine_bornmax(const fm_plan* P, double eps_imag, int itmax_setting) 
   return (int)std::ceil(std::sqrt(ext) / steps / 2.0 + 1.0) * 2 * std::abs(itmax_setting);
 }
 
-template <typename R>
+// One s-step block (fm_blockalg.cu) on every running block slot in its second phase, each at its own column m
+// (basis size m + 1): start vectors, s shifted operator applications on the FP64 block vectors, the block dot,
+// the in-place update and its Gram matrix, and the orthonormalised block stored after each slot's basis.
+template <typename R, typename YR>
+static fm_status engine_block_step(fm_engine* E, std::vector<int>& acth, const RhsCtx& rc) {
+  using T = cplx<R>;
+  using TY = cplx<YR>;
+  fm_plan* P = E->P;
+  const int S = E->S, bs = E->bs;
+  const size_t fe = (size_t)P->M;
+  std::vector<int> run;
+  for (int s = 0; s < S; ++s) {
+    const EngineSlot& sl = E->slots[s];
+    acth[s] = sl.state == SL_RUN && sl.blk && sl.phase == 2;
+    if (acth[s]) run.push_back(s);
+  }
+  if (run.empty()) return FM_OK;
+  const int nact = (int)run.size();
+  int* act = (int*)E->act.p;
+  T* U = (T*)E->U.p;
+  TY* Yb = (TY*)E->Yb.p;
+  FM_CK(cudaMemcpyAsync(act, acth.data(), S * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  // Y_0 = V_m of each slot (a combination of the stored vectors of m's diagonal block)
+  int Kmax = 0;
+  std::vector<int> kh(S, 0), k0h(S, 0), nch(S, 0);
+  std::vector<double2> cc((size_t)S * 16, make_double2(0, 0));
+  for (int s : run) {
+    const EngineSlot& sl = E->slots[s];
+    kh[s] = sl.m + 1;
+    k0h[s] = blk_start(sl.bst, sl.m, cc.data() + (size_t)s * 16);
+    nch[s] = sl.m - k0h[s] + 1;
+    Kmax = std::max(Kmax, kh[s]);
+  }
+  FM_CK(cudaMemcpyAsync(E->kbd.p, kh.data(), S * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  FM_CK(cudaMemcpyAsync(E->vrowd.p, kh.data(), S * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  FM_CK(cudaMemcpyAsync(E->k0d.p, k0h.data(), S * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  FM_CK(cudaMemcpyAsync(E->ncd.p, nch.data(), S * sizeof(int), cudaMemcpyHostToDevice, P->st));
+  FM_CK(cudaMemcpyAsync(P->coef.p, cc.data(), cc.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  double ncs = 0;
+  for (int s : run) ncs += nch[s];
+  FM_TRACK(P, KC_AXPBY, (ncs * sizeof(T) + nact * sizeof(TY)) * (double)fe,
+           (k_combine<R, TY><<<dim3(2 * P->sms, S), KV_THREADS, 0, P->st>>>(
+               P->M, S, 0, 1, U, (const double2*)P->coef.p, 16, Yb, act, (const int*)E->k0d.p,
+               (const int*)E->ncd.p)));
+  FM_CK(cudaGetLastError());
+  // Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}, t = 1..s, with each slot's potential and shifts
+  RhsCtx rcY = rc;
+  rcY.V = sizeof(TY) != sizeof(T) ? E->V64s.p : E->Vs.p;
+  EpiParams ep{};
+  ep.inv_eps = 1.0;
+  std::vector<double2> th(S, make_double2(0, 0));
+  for (int t = 1; t <= bs; ++t) {
+    for (int s : run)
+      th[s] = make_double2(E->slots[s].bst.theta[t - 1].real(), E->slots[s].bst.theta[t - 1].imag());
+    FM_CK(cudaMemcpyAsync(P->shifts.p, th.data(), S * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    EpiParams eps = ep;
+    eps.shift_b = (const double2*)P->shifts.p;
+    TY* Yin = Yb + (size_t)(t - 1) * S * fe;
+    TY* Yout = Yb + (size_t)t * S * fe;
+    FM_TRY(green_op<YR>(P, S, Yin, PRO_V, nullptr, EPI_PREC_OP, Yin, nullptr, eps, Yout, act, nact, &rcY));
+  }
+  // D = X^H Y_{1..s} (rows past each slot's basis come out zero)
+  const int* kbd = (const int*)E->kbd.p;
+  FM_CK((block_kernels<R, YR>(P, 0, bs, S, Kmax, U, Yb + (size_t)S * fe, nullptr, act, nact, kbd)));
+  std::vector<double2> D((size_t)S * Kmax * bs);
+  FM_CK(cudaMemcpyAsync(D.data(), P->red_out.p, D.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  tk_resolve(P);
+  std::vector<std::vector<cd>> Cv(S);
+  std::vector<double2> cf((size_t)S * KV_KMAX * bs, make_double2(0, 0));
+  for (int s : run)
+    blk_project(E->slots[s].bst, E->slots[s].m, bs, D.data() + (size_t)s * Kmax * bs, Cv[s],
+                cf.data() + (size_t)s * KV_KMAX * bs);
+  FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  // Y' = Y - X E in place, and its Gram matrix
+  FM_CK((block_kernels<R, YR>(P, 2, bs, S, Kmax, U, Yb + (size_t)S * fe, Yb + (size_t)S * fe, act, nact, kbd)));
+  const int NG = bs <= 8 ? bs * (bs + 1) / 2 : bs * bs;
+  std::vector<double2> Gt((size_t)S * NG);
+  FM_CK(cudaMemcpyAsync(Gt.data(), P->red_out.p, Gt.size() * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
+  FM_CK(cudaStreamSynchronize(P->st));
+  tk_resolve(P);
+  std::vector<double2> rbi((size_t)S * bs * bs, make_double2(0, 0));
+  for (int s : run) {
+    EngineSlot& sl = E->slots[s];
+    const bool stop = blk_absorb(sl.bst, sl.m, bs, true, Gt.data() + (size_t)s * NG, Cv[s],
+                                 rbi.data() + (size_t)s * bs * bs, sl.maxiters);
+    sl.iters = sl.bst.iters;
+    sl.rnorm = sl.bst.rnorm;
+    sl.solved = sl.bst.solved;
+    if (stop) sl.state = SL_STOP;
+    else sl.m += bs;
+  }
+  // V = Y' Rb^{-1} into each slot's basis rows m+1 .. m+s (also for slots that stopped in this block: their
+  // solution uses these vectors; a block that lost rank gets zero coefficients and is not used)
+  FM_CK(cudaMemcpyAsync(P->coef.p, rbi.data(), rbi.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  FM_CK((block_kernels<R, YR>(P, 3, bs, S, 0, U, Yb + (size_t)S * fe, U, act, nact, (const int*)E->vrowd.p)));
+  return FM_OK;
+}
+
+template <typename R, typename YR>
 static fm_status engine_step_t(fm_engine* E) {
   using T = cplx<R>;
+  using TY = cplx<YR>;
   fm_plan* P = E->P;
   const int S = E->S;
   const size_t M = (size_t)P->M, n = (size_t)P->n;
@@ -314,8 +458,14 @@ static fm_status engine_step_t(fm_engine* E) {
                                                     (const double*)P->fx.p, (const double*)P->fy.p,
                                                     (const double*)P->fz.p, 1.0 / kref2, (T*)E->Vs.p + (size_t)s * n);
       FM_CK(cudaGetLastError());
+      if (E->bs && sizeof(TY) != sizeof(T)) {  // the block vectors' operator reads an FP64 potential
+        k_to_f64<R><<<2 * P->sms, 256, 0, P->st>>>((long long)n, (const T*)E->Vs.p + (size_t)s * n, 1.0,
+                                                   (double2*)E->V64s.p + (size_t)s * n);
+        FM_CK(cudaGetLastError());
+      }
       // iteration limit of this right-hand side (convergent_born.jl:746)
       sl.maxiters = std::max(2 * engine_bornmax(P, sl.eps_imag, sl.u.itmax_setting), 100);
+      sl.blk = E->bs > 0 && sl.maxiters + E->bs + 1 <= E->mem + 1 && (M & 3) == 0;
       FM_TRY(wave_tables(P, sl.u.src, E->eps_bg, tx.data(), ty.data(), tz.data(), pe.data(), ph.data()));
       FM_CK(cudaMemcpyAsync((double2*)E->wt_x.p + (size_t)s * n3[0], tx.data(), n3[0] * sizeof(double2),
                             cudaMemcpyHostToDevice, P->st));
@@ -364,7 +514,15 @@ static fm_status engine_step_t(fm_engine* E) {
           sl.beta0 = sl.beta;
           sl.rnorm = sl.beta;
           sl.eps = sl.u.tol * 1e-2 + sl.u.tol * sl.beta;  // abstol + reltol * ||r0||
-          if (sl.beta == 0.0 || sl.rnorm <= sl.eps) {
+          if (sl.blk) {
+            sl.m = sl.j = 0;
+            sl.phase = 1;
+            if (blk_init(sl.bst, E->mem + 2, sl.beta, sl.u.tol * 1e-2, sl.u.tol)) {
+              sl.solved = true;
+              sl.state = SL_STOP;
+              continue;
+            }
+          } else if (sl.beta == 0.0 || sl.rnorm <= sl.eps) {
             sl.solved = true;
             sl.state = SL_STOP;
             continue;
@@ -380,9 +538,18 @@ static fm_status engine_step_t(fm_engine* E) {
     }
   }
 
-  // ---- 3. one GMRES iteration on every running slot ----
+  // ---- 3. one GMRES iteration on every running slot (block slots: their first s steps) ----
   {
     std::vector<int> run = select({SL_RUN});
+    for (size_t q = 0; q < run.size();) {
+      const EngineSlot& sl = E->slots[run[q]];
+      if (sl.blk && sl.phase == 2) {
+        acth[run[q]] = 0;
+        run.erase(run.begin() + q);
+      } else {
+        ++q;
+      }
+    }
     if (!run.empty()) {
       FM_TRY(upload_act());
       std::vector<const void*> tin(S, nullptr);
@@ -450,6 +617,26 @@ static fm_status engine_step_t(fm_engine* E) {
         std::vector<cd> col(K);
         for (int i = 0; i < K; ++i) col[i] = cd(htot[(size_t)s * kmax + i].x, htot[(size_t)s * kmax + i].y);
         const double hb = std::sqrt(std::max(0.0, nn[s].x));
+        if (sl.blk) {  // Hessenberg column m of the block solve, its Givens update and stop test
+          BlkState& r = sl.bst;
+          for (int i = 0; i < K; ++i) r.H[i + (size_t)sl.m * r.ld] = col[i];
+          const bool stop = blk_cgs_close(r, sl.m, hb, sl.maxiters);
+          sl.iters = r.iters;
+          sl.rnorm = r.rnorm;
+          sl.solved = r.solved;
+          if (stop) {
+            sl.state = SL_STOP;
+            continue;
+          }
+          E->sch[(size_t)(sl.m + 1) * S + s] = 1.0 / hb;
+          sl.j = ++sl.m;
+          if (sl.m == E->bs) {  // Newton shifts: Ritz values of the leading s x s Hessenberg block, Leja ordered
+            r.theta.assign(E->bs, 0.0);
+            blk_shifts(r, 0, E->bs);
+            sl.phase = 2;
+          }
+          continue;
+        }
         for (int i = 0; i < K - 1; ++i) {
           cd t = sl.c[i] * col[i] + sl.sn[i] * col[i + 1];
           col[i + 1] = std::conj(sl.sn[i]) * col[i] - sl.c[i] * col[i + 1];
@@ -482,6 +669,9 @@ static fm_status engine_step_t(fm_engine* E) {
     }
   }
 
+  // ---- 3b. one s-step block on every block slot past its first s steps ----
+  if (E->bs) FM_TRY((engine_block_step<R, YR>(E, acth, rc)));
+
   // ---- 4. x += sum_i y_i v_i for slots whose cycle ended ----
   {
     std::vector<int> upd = select({SL_STOP, SL_RESTART});
@@ -490,6 +680,13 @@ static fm_status engine_step_t(fm_engine* E) {
     int kmax = 0;
     for (int s : upd) {
       EngineSlot& sl = E->slots[s];
+      if (sl.blk) {  // X coordinates: the stored vectors enter unscaled
+        const int nv = blk_solution(sl.bst, yh.data() + (size_t)s * (KV_KMAX + 1));
+        for (int i = 0; i < nv; ++i) E->sch[(size_t)i * S + s] = 1.0;
+        kb[s] = nv;
+        kmax = std::max(kmax, nv);
+        continue;
+      }
       const int n_in = sl.inner;
       if (n_in == 0) continue;
       std::vector<cd> y(sl.z.begin(), sl.z.begin() + n_in);
@@ -562,7 +759,9 @@ fm_status fm_engine_step(fm_engine* E, int* n_done, long long* done_req, int* do
                          int max_done) {
   if (!E) return fail(FM_ERR_INVALID, "null engine");
   FM_CK(cudaSetDevice(E->P->desc.device));
-  fm_status st = E->P->prec == FM_PREC_F64 ? engine_step_t<double>(E) : engine_step_t<float>(E);
+  fm_status st = E->P->prec == FM_PREC_F64 ? engine_step_t<double, double>(E)
+                 : E->P->c64              ? engine_step_t<float, double>(E)
+                                          : engine_step_t<float, float>(E);
   if (st != FM_OK) return st;
   std::lock_guard<std::mutex> lk(E->mu);
   int k = 0;

@@ -192,6 +192,76 @@ __device__ __forceinline__ void fft_run(T (&v)[E], T* sm, const T* tw, int t) {
   }
 }
 
+// ---- NC pencils of one lane group run stage by stage together ----
+// Pencil c exchanges through its own buffer sm + c*SMS, so between two __syncwarp the loads and butterflies of
+// all NC pencils are independent and one pencil's exchange latency overlaps the others' arithmetic.  The stage
+// twiddles are loaded once, before any store of the stage, and shared by the NC pencils.
+template <int DIR, int L, int E, int RAD, int NS, bool LAST, int NC, int SMS, typename T>
+__device__ __forceinline__ void fft_stage_n(T (&v)[NC][E], T* sm, const T* tw, int t) {
+  constexpr int TP = L / E;
+  constexpr int NB = E / RAD;
+  static_assert(E % RAD == 0, "radix must divide E");
+  T w[NB][RAD - 1];
+  if constexpr (NS > 1) {
+#pragma unroll
+    for (int m = 0; m < NB; ++m)
+#pragma unroll
+      for (int q = 1; q < RAD; ++q) {
+        T a = tw[(NS - 1) + (q - 1) * NS + (t + TP * m) % NS];
+        if constexpr (DIR > 0) a = cconj(a);
+        w[m][q - 1] = a;
+      }
+  }
+#pragma unroll
+  for (int m = 0; m < NB; ++m) {
+    const int j = t + TP * m;
+    const int k = j % NS;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if constexpr (NS > 1) {
+#pragma unroll
+        for (int q = 1; q < RAD; ++q) v[c][m * RAD + q] = cmul(v[c][m * RAD + q], w[m][q - 1]);
+      }
+      bfly<DIR, RAD>(&v[c][m * RAD]);
+      if constexpr (!LAST) {
+        const int base = (j / NS) * NS * RAD + k;
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) sm[c * SMS + sm_phys<T>(base + q * NS)] = v[c][m * RAD + q];
+      }
+    }
+  }
+}
+
+template <int L, int E, int RAD, int NC, int SMS, typename T>
+__device__ __forceinline__ void fft_gather_n(T (&v)[NC][E], const T* sm, int t) {
+#pragma unroll
+  for (int c = 0; c < NC; ++c) fft_gather<L, E, RAD>(v[c], sm + c * SMS, t);
+}
+
+template <int DIR, int L, int E, int R0, int R1, int R2, int NC, int SMS, typename T>
+__device__ __forceinline__ void fft_run_n(T (&v)[NC][E], T* sm, const T* tw, int t) {
+  static_assert(R0 * (R1 ? R1 : 1) * (R2 ? R2 : 1) == L, "radices must multiply to L");
+  if constexpr (R1 == 0) {
+    fft_stage_n<DIR, L, E, R0, 1, true, NC, SMS>(v, sm, tw, t);
+  } else if constexpr (R2 == 0) {
+    fft_stage_n<DIR, L, E, R0, 1, false, NC, SMS>(v, sm, tw, t);
+    __syncwarp();
+    fft_gather_n<L, E, R1, NC, SMS>(v, sm, t);
+    __syncwarp();
+    fft_stage_n<DIR, L, E, R1, R0, true, NC, SMS>(v, sm, tw, t);
+  } else {
+    fft_stage_n<DIR, L, E, R0, 1, false, NC, SMS>(v, sm, tw, t);
+    __syncwarp();
+    fft_gather_n<L, E, R1, NC, SMS>(v, sm, t);
+    __syncwarp();
+    fft_stage_n<DIR, L, E, R1, R0, false, NC, SMS>(v, sm, tw, t);
+    __syncwarp();
+    fft_gather_n<L, E, R2, NC, SMS>(v, sm, t);
+    __syncwarp();
+    fft_stage_n<DIR, L, E, R2, R0 * R1, true, NC, SMS>(v, sm, tw, t);
+  }
+}
+
 // ---- per-length plans ----
 // E elements per lane and the forward radix sequence; TP = L/E lanes per pencil, 4 <= TP <= 32
 // (so at most 8 pencils share a warp and every axis of >= 8 points tiles a warp).
@@ -231,6 +301,18 @@ __device__ __forceinline__ void fft_rev_plan(T (&v)[P::E], T* sm, const T* tw_re
   if constexpr (P::R1 == 0) fft_run<DIR, P::L, P::E, P::R0, 0, 0>(v, sm, tw_rev, t);
   else if constexpr (P::R2 == 0) fft_run<DIR, P::L, P::E, P::R1, P::R0, 0>(v, sm, tw_rev, t);
   else fft_run<DIR, P::L, P::E, P::R2, P::R1, P::R0>(v, sm, tw_rev, t);
+}
+
+// NC pencils at once (exchange buffers SMS elements apart)
+template <int DIR, typename P, int NC, int SMS, typename T>
+__device__ __forceinline__ void fft_fwd_plan_n(T (&v)[NC][P::E], T* sm, const T* tw_fwd, int t) {
+  fft_run_n<DIR, P::L, P::E, P::R0, P::R1, P::R2, NC, SMS>(v, sm, tw_fwd, t);
+}
+template <int DIR, typename P, int NC, int SMS, typename T>
+__device__ __forceinline__ void fft_rev_plan_n(T (&v)[NC][P::E], T* sm, const T* tw_rev, int t) {
+  if constexpr (P::R1 == 0) fft_run_n<DIR, P::L, P::E, P::R0, 0, 0, NC, SMS>(v, sm, tw_rev, t);
+  else if constexpr (P::R2 == 0) fft_run_n<DIR, P::L, P::E, P::R1, P::R0, 0, NC, SMS>(v, sm, tw_rev, t);
+  else fft_run_n<DIR, P::L, P::E, P::R2, P::R1, P::R0, NC, SMS>(v, sm, tw_rev, t);
 }
 
 // Padded pencil stride in the exchange buffer.  A shared-memory wavefront serves

@@ -2,6 +2,7 @@
 // s-step block GMRES on the FP64 tensor cores, BiCGStab and the plain Born series -- and the solve core that
 // runs them from source terms to the scattered field and its curl.
 #include "fm_plan.cuh"
+#include "fm_blockalg.h"
 
 // ---------------------------------------------------------------------------
 // Krylov helpers
@@ -386,162 +387,18 @@ static fm_status gmres(fm_plan* P, int nb, const fm_solve_opts& o, std::vector<f
 // as in gmres() above, so the iteration at which a RHS stops and the iterate
 // it returns are those of full GMRES (in exact arithmetic).
 // ---------------------------------------------------------------------------
-namespace {
-
-// eigenvalues of an n x n complex upper Hessenberg matrix (column-major), shifted QR with deflation
-bool hess_eigs(int n, std::vector<cd> A, std::vector<cd>& ev) {
-  ev.clear();
-  auto a = [&](int i, int j) -> cd& { return A[i + (size_t)j * n]; };
-  int hi = n - 1, iter = 0;
-  while (hi >= 0) {
-    if (hi == 0) {
-      ev.push_back(a(0, 0));
-      break;
-    }
-    int l = hi;
-    while (l > 0 && std::abs(a(l, l - 1)) > 1e-15 * (std::abs(a(l, l)) + std::abs(a(l - 1, l - 1)))) --l;
-    if (l == hi) {
-      ev.push_back(a(hi, hi));
-      --hi;
-      iter = 0;
-      continue;
-    }
-    if (++iter > 100 * n) return false;
-    // Wilkinson shift from the trailing 2x2 block of the window [l, hi]
-    const cd p = a(hi - 1, hi - 1), q = a(hi - 1, hi), r = a(hi, hi - 1), t = a(hi, hi);
-    const cd tr = p + t, det = p * t - q * r, disc = std::sqrt(tr * tr / 4.0 - det);
-    const cd m1 = tr / 2.0 + disc, m2 = tr / 2.0 - disc;
-    cd mu = std::abs(m1 - t) < std::abs(m2 - t) ? m1 : m2;
-    if (iter % 11 == 10) mu += std::abs(a(hi, hi - 1));  // exceptional shift
-    std::vector<double> cs(hi - l);
-    std::vector<cd> sn(hi - l);
-    for (int k = l; k <= hi; ++k) a(k, k) -= mu;
-    for (int k = l; k < hi; ++k) {  // A - mu I = Q R, Givens G_k zeroes a(k+1, k)
-      const cd x = a(k, k), y = a(k + 1, k);
-      const double nr = std::sqrt(std::norm(x) + std::norm(y));
-      double c = 1.0;
-      cd sg = 0.0;
-      if (nr > 0) {
-        c = std::abs(x) / nr;
-        sg = (std::abs(x) > 0 ? x / std::abs(x) : cd(1.0, 0.0)) * std::conj(y) / nr;
-      }
-      for (int j = k; j <= hi; ++j) {
-        const cd t1 = a(k, j), t2 = a(k + 1, j);
-        a(k, j) = c * t1 + sg * t2;
-        a(k + 1, j) = -std::conj(sg) * t1 + c * t2;
-      }
-      cs[k - l] = c;
-      sn[k - l] = sg;
-    }
-    for (int k = l; k < hi; ++k) {  // R Q = R G_l^H ... G_{hi-1}^H
-      const double c = cs[k - l];
-      const cd sg = sn[k - l];
-      for (int i = l; i <= k + 1; ++i) {
-        const cd t1 = a(i, k), t2 = a(i, k + 1);
-        a(i, k) = c * t1 + std::conj(sg) * t2;
-        a(i, k + 1) = -sg * t1 + c * t2;
-      }
-    }
-    for (int k = l; k <= hi; ++k) a(k, k) += mu;
-  }
-  return true;
-}
-
-// Leja ordering: start from the largest modulus, then maximise the product of distances
-void leja_order(std::vector<cd>& z) {
-  std::vector<cd> out;
-  std::vector<bool> used(z.size(), false);
-  for (size_t n = 0; n < z.size(); ++n) {
-    int best = -1;
-    double bv = -1.0;
-    for (size_t i = 0; i < z.size(); ++i) {
-      if (used[i]) continue;
-      double v = 1.0;
-      if (out.empty()) v = std::abs(z[i]);
-      else
-        for (const cd& o : out) v *= std::abs(z[i] - o);
-      if (v > bv) {
-        bv = v;
-        best = (int)i;
-      }
-    }
-    used[best] = true;
-    out.push_back(z[best]);
-  }
-  z = out;
-}
-
-// G = R^H R for an n x n Hermitian positive definite G (column-major); false when not positive definite
-bool chol_upper(int n, const std::vector<cd>& G, std::vector<cd>& R) {
-  R.assign((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    cd d = G[j + (size_t)j * n];
-    for (int k = 0; k < j; ++k) d -= std::conj(R[k + (size_t)j * n]) * R[k + (size_t)j * n];
-    if (!(d.real() > 0.0) || !std::isfinite(d.real())) return false;
-    const double rd = std::sqrt(d.real());
-    R[j + (size_t)j * n] = rd;
-    for (int i = j + 1; i < n; ++i) {
-      cd v = G[j + (size_t)i * n];
-      for (int k = 0; k < j; ++k) v -= std::conj(R[k + (size_t)j * n]) * R[k + (size_t)i * n];
-      R[j + (size_t)i * n] = v / rd;
-    }
-  }
-  return true;
-}
-
-struct BlkState {
-  bool active = true, solved = false;
-  double beta = 0, eps = 0, rnorm = 0;
-  int iters = 0;            // Krylov iterations (Hessenberg columns) taken
-  int nvec = 0;             // stored basis vectors
-  int ld = 0;               // leading dimension of H and Rf
-  std::vector<cd> H;        // V-coordinate Hessenberg, H[i + j*ld]
-  std::vector<cd> Rf;       // X = V Rf, Rf[i + k*ld]
-  std::vector<int> b0;      // first index of the diagonal block of Rf that holds column k
-  std::vector<double> c;    // Givens
-  std::vector<cd> s, z;
-  std::vector<std::vector<cd>> Rg;
-  std::vector<cd> theta;    // Newton shifts
-};
-
-// d = Rf^{-1} c over the first K indices (K ends on a block boundary)
-void rf_solve(const BlkState& st, int K, const cd* c, cd* d) {
-  for (int k = K - 1; k >= 0;) {
-    const int a0 = st.b0[k];
-    for (int i = k; i >= a0; --i) {
-      cd v = c[i];
-      for (int j = i + 1; j <= k; ++j) v -= st.Rf[i + (size_t)j * st.ld] * d[j];
-      d[i] = v / st.Rf[i + (size_t)i * st.ld];
-    }
-    k = a0 - 1;
-  }
-}
-
-// d = Rf^{-H} c over the first K indices
-void rf_solve_h(const BlkState& st, int K, const cd* c, cd* d) {
-  for (int k0 = 0; k0 < K;) {
-    int k1 = k0;
-    while (k1 + 1 < K && st.b0[k1 + 1] == k0) ++k1;
-    for (int i = k0; i <= k1; ++i) {
-      cd v = c[i];
-      for (int j = k0; j < i; ++j) v -= std::conj(st.Rf[j + (size_t)i * st.ld]) * d[j];
-      d[i] = v / std::conj(st.Rf[i + (size_t)i * st.ld]);
-    }
-    k0 = k1 + 1;
-  }
-}
-
-}  // namespace
+// The per-RHS algebra (state, triangular solves, Hessenberg recovery, shifts, Givens) is in fm_blockalg.cu.
 
 
 template <typename R, typename YR, int S>
-static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, const void* Y, const int* act, int nact) {
+static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, const void* Y, const int* act, int nact,
+                                   const int* Kb) {
   using T = cplx<R>;
   using TY = cplx<YR>;
   const double bytes = ((double)K * sizeof(T) + (double)S * sizeof(TY)) * nact * P->M;
   const size_t pb =
       P->bd_bulk ? blockdot_bulk_part_bytes((int)sizeof(R), (int)sizeof(YR), S, P->M, nb, nact, K, P->sms) : 0;
-  if (pb) {
+  if (pb && !Kb) {
     cudaError_t e = P->red_part.ensure(pb);
     if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(K * S, KV_KMAX + 2) * sizeof(double2));
     if (e != cudaSuccess) return e;
@@ -568,7 +425,7 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
   FM_TRACK(P, KC_DOT, bytes,
            (kern<<<dim3(nblk, nb), threads, 0, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y,
                                                          (double2*)P->red_part.p, (double2*)P->red_out.p,
-                                                         (unsigned*)P->red_cnt.p, act)));
+                                                         (unsigned*)P->red_cnt.p, act, Kb)));
   return cudaGetLastError();
 }
 
@@ -578,7 +435,7 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
 // against itself on the tensor cores).
 template <typename R, typename YR, int S, typename TZ>
 static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, const void* Y, void* Z, const int* act,
-                                      int nact) {
+                                      int nact, const int* Kb) {
   using T = cplx<R>;
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
@@ -590,7 +447,7 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
   FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
            (kern<<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z,
-                                                            (const double2*)P->coef.p, act)));
+                                                            (const double2*)P->coef.p, act, Kb)));
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if constexpr (S > 8) {
@@ -606,7 +463,7 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
     FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
              (kern<<<dim3(nblk_g, nb), threads, 0, P->st>>>(P->M, nb, S, (const cplx<ZR>*)Z, (const TZ*)Z,
                                                              (double2*)P->red_part.p, (double2*)P->red_out.p,
-                                                             (unsigned*)P->red_cnt.p, act)));
+                                                             (unsigned*)P->red_cnt.p, act, nullptr)));
     return cudaGetLastError();
   } else {
     const int nblk_g = kv_blocks(P, k_blockgram<R, S, TZ>, nb);
@@ -622,27 +479,28 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
 
 // V (basis slots) = Z Rb^{-1} for the orthonormalised block storage; coefficients in P->coef
 template <typename R, typename YR, int S>
-static cudaError_t launch_blocknorm(fm_plan* P, int nb, const void* Z, void* V, const int* act, int nact) {
+static cudaError_t launch_blocknorm(fm_plan* P, int nb, const void* Z, void* V, const int* act, int nact,
+                                    const int* vrow) {
   using T = cplx<R>;
   using TY = cplx<YR>;
   FM_TRACK(P, KC_AXPBY, (double)S * (sizeof(TY) + sizeof(T)) * nact * P->M,
            (k_blocknorm<R, TY, S><<<dim3(kv_blocks(P, k_blocknorm<R, TY, S>, nb), nb), KV_THREADS, 0, P->st>>>(
-               P->M, nb, (const TY*)Z, (const double2*)P->coef.p, (T*)V, act)));
+               P->M, nb, (const TY*)Z, (const double2*)P->coef.p, (T*)V, act, vrow)));
   return cudaGetLastError();
 }
 
-// which: 0 block dot, 1 block update into the basis, 2 block update in place into Y, 3 orthonormalisation
+// (declared in fm_plan.cuh)
 template <typename R, typename YR>
-static cudaError_t block_kernels(fm_plan* P, int which, int S, int nb, int K, const void* U, const void* Y, void* Z,
-                                 const int* act, int nact) {
+cudaError_t block_kernels(fm_plan* P, int which, int S, int nb, int K, const void* U, const void* Y, void* Z,
+                          const int* act, int nact, const int* Kb) {
   using T = cplx<R>;
   using TY = cplx<YR>;
 #define FM_BLK(SS)                                                                                     \
   case SS:                                                                                             \
-    return which == 0   ? launch_blockdot<R, YR, SS>(P, nb, K, U, Y, act, nact)                        \
-           : which == 1 ? launch_blockupdate<R, YR, SS, T>(P, nb, K, U, Y, Z, act, nact)              \
-           : which == 2 ? launch_blockupdate<R, YR, SS, TY>(P, nb, K, U, Y, Z, act, nact)             \
-                        : launch_blocknorm<R, YR, SS>(P, nb, Y, Z, act, nact);
+    return which == 0   ? launch_blockdot<R, YR, SS>(P, nb, K, U, Y, act, nact, Kb)                    \
+           : which == 1 ? launch_blockupdate<R, YR, SS, T>(P, nb, K, U, Y, Z, act, nact, Kb)          \
+           : which == 2 ? launch_blockupdate<R, YR, SS, TY>(P, nb, K, U, Y, Z, act, nact, Kb)         \
+                        : launch_blocknorm<R, YR, SS>(P, nb, Y, Z, act, nact, Kb);
   switch (S) {
     FM_BLK(2) FM_BLK(3) FM_BLK(4) FM_BLK(5) FM_BLK(6) FM_BLK(7) FM_BLK(8) FM_BLK(16)
     default: return cudaErrorInvalidValue;
@@ -687,7 +545,6 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
   }
   double* sc = (double*)P->scale.p;
   int* act = (int*)P->active.p;
-  const double btol = std::pow(2.220446049250313e-16, 0.75);
   const int ld = cap + 1;
 
   std::vector<BlkState> St(nb);
@@ -703,33 +560,6 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     for (int b = 0; b < nb; ++b) n += acth[b];
     return n;
   };
-  // Givens update with Hessenberg column j of RHS r; true when the RHS stops at this column
-  auto givens_col = [&](BlkState& r, int j) -> bool {
-    const int K = j + 1;
-    std::vector<cd> col(K);
-    for (int i = 0; i < K; ++i) col[i] = r.H[i + (size_t)j * ld];
-    const double hb = r.H[(j + 1) + (size_t)j * ld].real();
-    for (int i = 0; i < K - 1; ++i) {
-      cd t = r.c[i] * col[i] + r.s[i] * col[i + 1];
-      col[i + 1] = std::conj(r.s[i]) * col[i] - r.c[i] * col[i + 1];
-      col[i] = t;
-    }
-    double c;
-    cd sn, rho;
-    sym_givens(col[K - 1], hb, c, sn, rho);
-    col[K - 1] = rho;
-    r.c.push_back(c);
-    r.s.push_back(sn);
-    r.Rg.push_back(col);
-    const cd zk1 = std::conj(sn) * r.z[K - 1];
-    r.z[K - 1] = c * r.z[K - 1];
-    r.rnorm = std::abs(zk1);
-    r.iters = K;
-    r.solved = (r.rnorm <= r.eps) || (r.rnorm + 1.0 <= 1.0);
-    if (r.solved || hb <= btol || K >= itmax) return true;
-    r.z.push_back(zk1);
-    return false;
-  };
 
   // r0 = M^{-1}(b - A x) into X_0
   FM_TRY(upload_active());
@@ -737,24 +567,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
   std::vector<double2> hv;
   FM_TRY(multidot<R>(P, nb, 0, U, U, true, act, hv));
   for (int b = 0; b < nb; ++b) {
-    BlkState& r = St[b];
-    r.ld = ld;
-    r.H.assign((size_t)ld * ld, 0.0);
-    r.Rf.assign((size_t)ld * ld, 0.0);
-    r.b0.assign(ld, 0);
-    r.beta = std::sqrt(hv[b].x);
-    r.rnorm = r.beta;
-    r.eps = o.abstol + o.reltol * r.beta;
-    info[b].residual0 = r.beta;
-    r.Rf[0] = r.beta;
-    r.b0[0] = 0;
-    r.nvec = 1;
-    r.z.assign(1, cd(r.beta, 0.0));
-    if (r.beta == 0.0 || r.rnorm <= r.eps) {
-      r.active = false;
-      r.solved = true;
-      acth[b] = 0;
-    }
+    if (blk_init(St[b], ld, std::sqrt(hv[b].x), o.abstol, o.reltol)) acth[b] = 0;
+    info[b].residual0 = St[b].beta;
   }
 
   // ---- phase 1: S classical Gram-Schmidt steps (Ritz values for the shifts) ----
@@ -772,16 +586,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     std::vector<double2> hr;
     FM_TRY(multidot<R>(P, nb, K, U, Uw, false, act, hr, nact));
     std::vector<double2> cf((size_t)nb * K, make_double2(0, 0));
-    for (int b = 0; b < nb; ++b) {
-      if (!acth[b]) continue;
-      for (int k = 0; k < K; ++k) {
-        const double rk = St[b].Rf[k + (size_t)k * ld].real();
-        const cd h = cd(hr[(size_t)b * K + k].x, hr[(size_t)b * K + k].y) / rk;
-        St[b].H[k + (size_t)m * ld] = h;
-        const cd e = h / rk;
-        cf[(size_t)b * K + k] = make_double2(e.real(), e.imag());
-      }
-    }
+    for (int b = 0; b < nb; ++b)
+      if (acth[b]) blk_cgs_coefs(St[b], m, hr.data() + (size_t)b * K, cf.data() + (size_t)b * K);
     FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
     Coef c{(const double2*)P->coef.p, K, nullptr, nb, -1.0, 0};
     dim3 g(kv_blocks(P, k_update<R, true>, nb), nb);
@@ -793,34 +599,18 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     FM_CK(cudaMemcpyAsync(nn.data(), P->red_out.p, nb * sizeof(double2), cudaMemcpyDeviceToHost, P->st));
     FM_CK(cudaStreamSynchronize(P->st));
     tk_resolve(P);
-    for (int b = 0; b < nb; ++b) {
-      if (!acth[b]) continue;
-      BlkState& r = St[b];
-      const double hb = std::sqrt(std::max(0.0, nn[b].x));
-      r.H[(m + 1) + (size_t)m * ld] = hb;
-      r.Rf[(m + 1) + (size_t)(m + 1) * ld] = hb;
-      r.b0[m + 1] = m + 1;
-      r.nvec = m + 2;
-      if (givens_col(r, m)) {
-        r.active = false;
+    for (int b = 0; b < nb; ++b)
+      if (acth[b] && blk_cgs_close(St[b], m, std::sqrt(std::max(0.0, nn[b].x)), itmax)) {
+        St[b].active = false;
         acth[b] = 0;
       }
-    }
     ++m;
     if (deadline > 0 && now_s() > deadline) return fail(FM_ERR_TIMEOUT, "solve deadline passed");
   }
   // Newton shifts: Ritz values of the leading S x S Hessenberg block, Leja ordered
   for (int b = 0; b < nb; ++b) {
-    BlkState& r = St[b];
-    r.theta.assign(S, 0.0);
-    if (!r.active) continue;
-    std::vector<cd> Hs((size_t)S * S), ev;
-    for (int j = 0; j < S; ++j)
-      for (int i = 0; i < S; ++i) Hs[i + (size_t)j * S] = r.H[i + (size_t)j * ld];
-    if (hess_eigs(S, Hs, ev) && (int)ev.size() == S) {
-      leja_order(ev);
-      r.theta = ev;
-    }
+    St[b].theta.assign(S, 0.0);
+    if (St[b].active) blk_shifts(St[b], 0, S);
   }
 
   // ---- phase 2: s-step blocks ----
@@ -830,18 +620,11 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     const int K = m + 1;
     // Y_0 = V_m = sum_k X_k (Rf^{-1})_{k,m} over m's diagonal block (the same block layout for every RHS)
     int k0 = m;
-    for (int b = 0; b < nb; ++b)
-      if (acth[b]) k0 = St[b].b0[m];
-    const int nc = m - k0 + 1;
     {
       std::vector<double2> cc((size_t)nb * 16, make_double2(0, 0));
-      for (int b = 0; b < nb; ++b) {
-        if (!acth[b]) continue;
-        std::vector<cd> em(K, 0.0), d(K, 0.0);
-        em[m] = 1.0;
-        rf_solve(St[b], K, em.data(), d.data());
-        for (int a2 = 0; a2 < nc; ++a2) cc[(size_t)b * 16 + a2] = make_double2(d[k0 + a2].real(), d[k0 + a2].imag());
-      }
+      for (int b = 0; b < nb; ++b)
+        if (acth[b]) k0 = blk_start(St[b], m, cc.data() + (size_t)b * 16);
+      const int nc = m - k0 + 1;
       FM_CK(cudaMemcpyAsync(P->coef.p, cc.data(), cc.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
       FM_TRACK(P, KC_AXPBY, (double)nc * nact * fe * sizeof(T) + (double)nact * fe * sizeof(TY),
                (k_combine<R, TY><<<dim3(2 * P->sms, nb), KV_THREADS, 0, P->st>>>(
@@ -869,23 +652,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     // C = Rf^{-H} D (V coordinates), E = Rf^{-1} C (X coordinates) for the update
     std::vector<std::vector<cd>> Cv(nb);
     std::vector<double2> cf((size_t)nb * KV_KMAX * S, make_double2(0, 0));
-    for (int b = 0; b < nb; ++b) {
-      if (!acth[b]) continue;
-      Cv[b].assign((size_t)K * S, 0.0);
-      std::vector<cd> dcol(K), ccol(K), ecol(K);
-      for (int t = 0; t < S; ++t) {
-        for (int k = 0; k < K; ++k) {
-          const double2 v = D[((size_t)b * K + k) * S + t];
-          dcol[k] = cd(v.x, v.y);
-        }
-        rf_solve_h(St[b], K, dcol.data(), ccol.data());
-        rf_solve(St[b], K, ccol.data(), ecol.data());
-        for (int k = 0; k < K; ++k) {
-          Cv[b][k + (size_t)t * K] = ccol[k];
-          cf[(size_t)b * KV_KMAX * S + (size_t)k * S + t] = make_double2(ecol[k].real(), ecol[k].imag());
-        }
-      }
-    }
+    for (int b = 0; b < nb; ++b)
+      if (acth[b]) blk_project(St[b], m, S, D.data() + (size_t)b * K * S, Cv[b], cf.data() + (size_t)b * KV_KMAX * S);
     FM_CK(cudaMemcpyAsync(P->coef.p, cf.data(), cf.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
     // Y' = Y - X E into basis slots m+1..m+S (orthonormalised storage: over Y in place), Gram of Y'
     if (ortho_store)
@@ -899,94 +667,10 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
     FM_CK(cudaStreamSynchronize(P->st));
     tk_resolve(P);
     std::vector<double2> rbi(ortho_store ? (size_t)nb * S * S : 0, make_double2(0, 0));
-    for (int b = 0; b < nb; ++b) {
-      if (!acth[b]) continue;
-      BlkState& r = St[b];
-      std::vector<cd> G((size_t)S * S), Rb;
-      int gi = 0;
-      for (int t = 0; t < S; ++t)
-        for (int u = t; u < S; ++u, ++gi) {
-          const size_t at = (size_t)b * NG + (S <= 8 ? (size_t)gi : (size_t)t * S + u);
-          const cd v(Gt[at].x, Gt[at].y);
-          G[t + (size_t)u * S] = v;
-          G[u + (size_t)t * S] = std::conj(v);
-        }
-      if (!chol_upper(S, G, Rb)) {  // the block lost rank: Krylov breakdown, keep the columns so far
-        r.active = false;
+    for (int b = 0; b < nb; ++b)
+      if (acth[b] && blk_absorb(St[b], m, S, ortho_store, Gt.data() + (size_t)b * NG, Cv[b],
+                                ortho_store ? rbi.data() + (size_t)b * S * S : nullptr, itmax))
         acth[b] = 0;
-        continue;
-      }
-      if (ortho_store) {
-        // stored columns V = Y' Rb^{-1} are orthonormal: identity diagonal blocks of Rf
-        for (int t = 0; t < S; ++t) {
-          std::vector<cd> col(S, 0.0);
-          col[t] = 1.0;
-          for (int i = t; i >= 0; --i) {
-            cd v = col[i];
-            for (int q = i + 1; q <= t; ++q) v -= Rb[i + (size_t)q * S] * col[q];
-            col[i] = v / Rb[i + (size_t)i * S];
-          }
-          for (int u = 0; u <= t; ++u) rbi[(size_t)b * S * S + u * S + t] = make_double2(col[u].real(), col[u].imag());
-        }
-        for (int u = 0; u < S; ++u) {
-          for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = (a == u) ? cd(1.0, 0.0) : cd(0.0, 0.0);
-          r.b0[K + u] = K + u;
-        }
-      } else {
-        for (int u = 0; u < S; ++u) {
-          for (int a = 0; a <= u; ++a) r.Rf[(K + a) + (size_t)(K + u) * ld] = Rb[a + (size_t)u * S];
-          r.b0[K + u] = K;
-        }
-      }
-      r.nvec = K + S;
-      // W: V coordinates of Y_0..Y_S, n x (S+1)
-      const int n = K + S;
-      std::vector<cd> W((size_t)n * (S + 1), 0.0);
-      W[m] = 1.0;  // Y_0 = V_m
-      for (int t = 0; t < S; ++t) {
-        for (int i = 0; i < K; ++i) W[i + (size_t)(t + 1) * n] = Cv[b][i + (size_t)t * K];
-        for (int a = 0; a < S; ++a) W[K + a + (size_t)(t + 1) * n] = Rb[a + (size_t)t * S];
-      }
-      // Rh = W[:,1:S] + W[:,0:S-1] diag(theta) - [H_{0:m,0:m-1} W_{0:m-1,0:S-1}; 0]
-      std::vector<cd> Rh((size_t)n * S), Hn((size_t)n * S);
-      for (int c = 0; c < S; ++c) {
-        for (int i = 0; i < n; ++i) Rh[i + (size_t)c * n] = W[i + (size_t)(c + 1) * n] + r.theta[c] * W[i + (size_t)c * n];
-        for (int j = 0; j < m; ++j) {
-          const cd w = W[j + (size_t)c * n];
-          if (w == cd(0.0, 0.0)) continue;
-          for (int i = 0; i <= j + 1; ++i) Rh[i + (size_t)c * n] -= r.H[i + (size_t)j * ld] * w;
-        }
-      }
-      // Hn = Rh T^{-1}, T = W[m..m+S-1, 0..S-1] upper triangular
-      for (int c = 0; c < S; ++c)
-        for (int i = 0; i < n; ++i) {
-          cd v = Rh[i + (size_t)c * n];
-          for (int a = 0; a < c; ++a) v -= Hn[i + (size_t)a * n] * W[m + a + (size_t)c * n];
-          Hn[i + (size_t)c * n] = v / W[m + c + (size_t)c * n];
-        }
-      for (int c = 0; c < S; ++c)
-        for (int i = 0; i < n; ++i) r.H[i + (size_t)(m + c) * ld] = (i <= m + c + 1) ? Hn[i + (size_t)c * n] : cd(0.0, 0.0);
-      // Newton shifts of the next block: Ritz values of this block's S x S diagonal Hessenberg block, Leja ordered.
-      // Shifts kept from the first S steps only let the basis of a later block lose conditioning; refreshed ones
-      // keep it near that of s = 4 up to s = 16 (a numpy restatement with FP32-rounded basis vectors on the CBS
-      // operator: 4.6e-6 -> 6e-8 at s = 8).
-      {
-        std::vector<cd> Hs((size_t)S * S), ev;
-        for (int j = 0; j < S; ++j)
-          for (int i = 0; i < S; ++i) Hs[i + (size_t)j * S] = r.H[(m + i) + (size_t)(m + j) * ld];
-        if (hess_eigs(S, Hs, ev) && (int)ev.size() == S) {
-          leja_order(ev);
-          r.theta = ev;
-        }
-      }
-      for (int c = 0; c < S; ++c) {
-        if (givens_col(r, m + c)) {
-          r.active = false;
-          acth[b] = 0;
-          break;
-        }
-      }
-    }
     if (ortho_store) {  // zero coefficients for right-hand sides whose block broke down: their slots stay unused
       FM_CK(cudaMemcpyAsync(P->coef.p, rbi.data(), rbi.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
       FM_CK((block_kernels<R, YR>(P, 3, S, nb, K, U, Yb + (size_t)nb * fe, U + (size_t)K * nb * fe, act, nact)));
@@ -998,25 +682,7 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
   // ---- x += V y = X Rf^{-1} y ----
   std::vector<double2> yh((size_t)nb * KV_KMAX, make_double2(0, 0));
   int Kmax = 0;
-  for (int b = 0; b < nb; ++b) {
-    BlkState& r = St[b];
-    const int n_in = r.iters;
-    if (n_in == 0) continue;
-    std::vector<cd> y(r.z.begin(), r.z.begin() + n_in);
-    for (int i = n_in - 1; i >= 0; --i) {
-      for (int jj = n_in - 1; jj > i; --jj) y[i] -= r.Rg[jj][i] * y[jj];
-      if (std::abs(r.Rg[i][i]) <= btol) {
-        for (int q = 0; q <= i; ++q) y[q] = 0.0;
-        break;
-      }
-      y[i] /= r.Rg[i][i];
-    }
-    std::vector<cd> yv(r.nvec, 0.0), d(r.nvec, 0.0);
-    for (int i = 0; i < n_in; ++i) yv[i] = y[i];
-    rf_solve(r, r.nvec, yv.data(), d.data());
-    for (int i = 0; i < r.nvec; ++i) yh[(size_t)b * KV_KMAX + i] = make_double2(d[i].real(), d[i].imag());
-    Kmax = std::max(Kmax, r.nvec);
-  }
+  for (int b = 0; b < nb; ++b) Kmax = std::max(Kmax, blk_solution(St[b], yh.data() + (size_t)b * KV_KMAX));
   if (Kmax > 0) {
     FM_CK(cudaMemcpyAsync(P->coef.p, yh.data(), yh.size() * sizeof(double2), cudaMemcpyHostToDevice, P->st));
     Coef cf{(const double2*)P->coef.p, KV_KMAX, nullptr, nb, 1.0, 1};
@@ -1238,3 +904,9 @@ template fm_status axpby3<double>(fm_plan*, int, const void*, const std::vector<
                                   const int*, std::vector<double>*);
 template fm_status solve_core<float>(fm_plan*, int, const fm_solve_opts&, std::vector<fm_solve_info>&);
 template fm_status solve_core<double>(fm_plan*, int, const fm_solve_opts&, std::vector<fm_solve_info>&);
+template cudaError_t block_kernels<float, double>(fm_plan*, int, int, int, int, const void*, const void*, void*,
+                                                  const int*, int, const int*);
+template cudaError_t block_kernels<double, double>(fm_plan*, int, int, int, int, const void*, const void*, void*,
+                                                   const int*, int, const int*);
+template cudaError_t block_kernels<float, float>(fm_plan*, int, int, int, int, const void*, const void*, void*,
+                                                 const int*, int, const int*);

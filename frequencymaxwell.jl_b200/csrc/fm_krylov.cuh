@@ -291,13 +291,18 @@ __global__ void __launch_bounds__(KV_THREADS) k_mgs(long long M, int B, int i, i
 // basis type).  M must be a multiple of 4.
 // ---------------------------------------------------------------------------
 
-// out[b] = sum_{a<n} c[b*cs + a] * X_{k0+a}[b]   (FP64 accumulation)
+// out[b] = sum_{a<n} c[b*cs + a] * X_{k0+a}[b]   (FP64 accumulation; n <= 16).  Optional per-RHS k0b[b], nb[b]
+// replace k0 and n.
 template <typename R, typename TY>
 __global__ void __launch_bounds__(KV_THREADS) k_combine(long long M, int B, int k0, int n, const cplx<R>* __restrict__ U,
                                                         const double2* __restrict__ c, int cs, TY* __restrict__ out,
-                                                        const int* __restrict__ active) {
+                                                        const int* __restrict__ active,
+                                                        const int* __restrict__ k0b = nullptr,
+                                                        const int* __restrict__ nb = nullptr) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
+  if (k0b) k0 = k0b[b];
+  if (nb) n = nb[b];
   __shared__ double2 cc[16];
   if (threadIdx.x < n) cc[threadIdx.x] = c[(size_t)b * cs + threadIdx.x];
   __syncthreads();
@@ -347,7 +352,8 @@ __device__ __forceinline__ void mma_f64(double& c0, double& c1, double a, double
                : "d"(a), "d"(b));
 }
 
-// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 16)
+// D[b][k*S + t] = sum_e conj(X_k[e]) * Y_t[e]   (FP64 tensor cores, deterministic; S <= 16).  Optional per-RHS
+// basis sizes Kb[b] <= K: the rows k >= Kb[b] of RHS b come out zero (the output keeps the stride K*S).
 // S <= 4: one B tile; S > 4: NTH = ceil(S/8) tiles of real parts then NTH tiles of imaginary parts (tile h holds
 // block vectors 8h .. 8h+7 in its columns), so that for t = 8h + c
 //   Re = P[h][c] + Q[NTH + h][c],  Im = P[NTH + h][c] - Q[h][c]  within each lane.
@@ -358,7 +364,8 @@ template <typename R, typename TY, int S, bool WIDE = false>
 __global__ void __launch_bounds__(KV_THREADS, (S > 8 || WIDE) ? 2 : 1) k_blockdot_mma(long long M, int B, int K, const cplx<R>* __restrict__ U,
                                                              const TY* __restrict__ Y, double2* __restrict__ part,
                                                              double2* __restrict__ out, unsigned* __restrict__ counter,
-                                                             const int* __restrict__ active) {
+                                                             const int* __restrict__ active,
+                                                             const int* __restrict__ Kb = nullptr) {
   static_assert(S >= 1 && S <= 16, "block dot on tensor cores takes 1..16 block vectors");
   static_assert(!WIDE || (S > 4 && S <= 8), "the wide form is for 5..8 block vectors");
   using T = cplx<R>;
@@ -376,6 +383,7 @@ __global__ void __launch_bounds__(KV_THREADS, (S > 8 || WIDE) ? 2 : 1) k_blockdo
   // as 32 * KW * EW threads (at most KV_THREADS) so that no warp idles
   const int KG = (K + 7) >> 3, KW = (KG + GPW - 1) / GPW, EW = (int)(blockDim.x >> 5) / KW;
   const int kw = w % KW, ew = w / KW;
+  const int Kr = Kb ? Kb[b] : K;  // basis vectors of this RHS
   double P[GPW][NT][2], Q[GPW][NT][2];
 #pragma unroll
   for (int g = 0; g < GPW; ++g)
@@ -416,7 +424,7 @@ __global__ void __launch_bounds__(KV_THREADS, (S > 8 || WIDE) ? 2 : 1) k_blockdo
       }
 #pragma unroll
       for (int g = 0; g < GPW; ++g) {
-        if ((kw * GPW + g) >= KG) break;  // warp-uniform
+        if ((kw * GPW + g) * 8 >= Kr) break;  // warp-uniform
         const int k = (kw * GPW + g) * 8 + gid;
         T xv[HR][4];
 #pragma unroll
@@ -426,7 +434,7 @@ __global__ void __launch_bounds__(KV_THREADS, (S > 8 || WIDE) ? 2 : 1) k_blockdo
             xv[h][q].x = 0;
             xv[h][q].y = 0;
           }
-          if (k < K && ein[h]) load4(ub + (size_t)k * us + e0 + 16 * h + 4 * tig, xv[h]);
+          if (k < Kr && ein[h]) load4(ub + (size_t)k * us + e0 + 16 * h + 4 * tig, xv[h]);
         }
 #pragma unroll
         for (int h = 0; h < HR; ++h)
@@ -499,12 +507,13 @@ __device__ __forceinline__ void load_run(const C* p, C (&v)[QR]) {
 // Z_t[b] = Y_t[b] - sum_k E[b][k*S + t] * X_k[b]  (FP64 tensor cores; S <= 16).  A warp owns 8*QR elements (lane
 // gid: elements QR gid .. QR gid + QR - 1 of the tile) and runs over the basis 4 vectors at a time.  B tiles as in
 // k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or, for t = 8h + c,
-// Re = P[h][c] - Q[NTH + h][c],  Im = P[NTH + h][c] + Q[h][c].
+// Re = P[h][c] - Q[NTH + h][c],  Im = P[NTH + h][c] + Q[h][c].  Optional per-RHS basis sizes Kb[b] <= K.
 template <typename R, typename TY, int S, typename TZ = cplx<R>>
 __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, TZ* Z,
                                                                 const double2* __restrict__ coef,
-                                                                const int* __restrict__ active) {
+                                                                const int* __restrict__ active,
+                                                                const int* __restrict__ Kb = nullptr) {
   static_assert(S >= 1 && S <= 16, "block update on tensor cores takes 1..16 block vectors");
   using T = cplx<R>;
   constexpr int NTH = S <= 4 ? 1 : (S + 7) / 8;
@@ -514,6 +523,7 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
   __shared__ double Bs[KV_KMAX][8 * NT];
   const int b = blockIdx.y;
   if (active && !active[b]) return;
+  if (Kb) K = Kb[b];
   for (int i = threadIdx.x; i < KV_KMAX * 8 * NT; i += blockDim.x) {
     const int k = i / (8 * NT), col = i - k * (8 * NT);
     int t;
@@ -678,7 +688,8 @@ __global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, co
 template <typename R, typename TZ, int S>
 __global__ void __launch_bounds__(KV_THREADS, 2) k_blocknorm(long long M, int B, const TZ* __restrict__ Z,
                                                           const double2* __restrict__ c, cplx<R>* __restrict__ V,
-                                                          const int* __restrict__ active) {
+                                                          const int* __restrict__ active,
+                                                          const int* __restrict__ vrow = nullptr) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   // coefficients are re-read from shared memory in the loop (volatile): held in registers they would take
@@ -693,7 +704,7 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blocknorm(long long M, int B,
   __syncthreads();
   const size_t us = (size_t)B * M;
   const TZ* zb = Z + (size_t)b * M;
-  cplx<R>* vb = V + (size_t)b * M;
+  cplx<R>* vb = V + (vrow ? (size_t)vrow[b] * us : 0) + (size_t)b * M;  // per-RHS first row (optional)
 #pragma unroll 1
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < M; e += (long long)gridDim.x * blockDim.x) {
     double2 z[S];

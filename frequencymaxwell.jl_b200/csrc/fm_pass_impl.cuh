@@ -275,6 +275,7 @@ template <typename S, typename R, int L, int MODE>
 static cudaError_t zg_tma_L(const Dims& d, const void* in, const GreenParams& gp, const void* tw, const void* rz,
                             void* out, const int* act, int* err, int sms, cudaStream_t st) {
   using C = ZTmaCfg<S, R, L, MODE>;
+  static_assert(C::SM::total <= 232448, "z pass shared memory above the 227 KB a CTA can have");
   if (d.nx % C::TX) return cudaErrorNotSupported;
   CUtensorMap mi, mo;
   if (!make_map(&mi, const_cast<void*>(in), d, (int)sizeof(cplx<S>), 4, 1, L) ||

@@ -176,7 +176,10 @@ struct ZTmaCfg {
   static constexpr int TILE = 3 * L * 128;
   static constexpr int NST = TILE <= 32768 ? 3 : 2;
   static constexpr int STRIDE = PencilStride<LF, T, P::TP, true>::v;
-  using SM = TmaSmem<TILE, NST, CW * PW * STRIDE * (int)sizeof(T), (2 * LF + L) * (int)sizeof(T)>;
+  // exchange buffers per pencil: the three components of a length-256 transform run stage by stage together
+  // (their exchanges overlap), each with its own buffer; shorter transforms run one component at a time
+  static constexpr int NCX = LF >= 256 ? 3 : 1;
+  using SM = TmaSmem<TILE, NST, CW * PW * NCX * STRIDE * (int)sizeof(T), (2 * LF + L) * (int)sizeof(T)>;
   static constexpr int THREADS = CW * 32;
 };
 
@@ -227,7 +230,8 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
     }
   }
   const int p = lane / TP, t = lane % TP;
-  T* sm = ex + (warp * PW + p) * C::STRIDE;
+  constexpr int NCX = C::NCX, SMS = C::STRIDE;
+  T* sm = ex + (warp * PW + p) * NCX * SMS;
   const R ksr = (R)gp.ksq_re;
   const T sc = mk((R)gp.scale_re, (R)gp.scale_im);
   int it = 0;
@@ -261,7 +265,13 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
           }
           v[c][e] = a;
         }
-        fft_fwd_plan<-1, P_>(v[c], sm, tw, t);
+        if constexpr (NCX == 1) {
+          fft_fwd_plan<-1, P_>(v[c], sm, tw, t);
+          __syncwarp();
+        }
+      }
+      if constexpr (NCX == 3) {
+        fft_fwd_plan_n<-1, P_, 3, SMS>(v, sm, tw, t);
         __syncwarp();
       }
       R kx, ky;
@@ -302,10 +312,16 @@ __global__ void __launch_bounds__(ZTmaCfg<S, R, L, MODE>::THREADS)
           v[2][e] = cmul(csub(e3, cscale(kE, kz)), f);
         }
       }
+      if constexpr (NCX == 3) {
+        fft_rev_plan_n<+1, P_, 3, SMS>(v, sm, twr, t);
+        __syncwarp();
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        fft_rev_plan<+1, P_>(v[c], sm, twr, t);
-        __syncwarp();
+        if constexpr (NCX == 1) {
+          fft_rev_plan<+1, P_>(v[c], sm, twr, t);
+          __syncwarp();
+        }
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           const int z = lay_idx<LF, E, P_::R0>(t, e);

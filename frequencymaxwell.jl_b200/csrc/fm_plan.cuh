@@ -371,6 +371,12 @@ fm_status axpby3(fm_plan* P, int nb, const void* a, const std::vector<cd>& ca, c
                  const std::vector<cd>& cbv, const void* c, const std::vector<cd>& ccv, void* y, bool norm,
                  const int* act, std::vector<double>* norms);
 void sym_givens(cd a, double b, double& c, cd& s, cd& rho);
+// Block Gram-Schmidt kernels on the FP64 tensor cores.  which: 0 block dot D = X^H Y, 1 block update into the
+// basis, 2 block update in place into Y, 3 orthonormalisation V = Z Rb^{-1}.  Kb (optional, device): per-RHS
+// basis sizes <= K for 0-2, and for 3 the per-RHS first basis row of the output (Z then points at row 0).
+template <typename R, typename YR>
+cudaError_t block_kernels(fm_plan* P, int which, int S, int nb, int K, const void* U, const void* Y, void* Z,
+                          const int* act, int nact, const int* Kb = nullptr);
 // vectors per block of block GMRES (fm_solve_opts.block; 0 selects 4)
 inline int block_size_of(const fm_solve_opts& o) { return o.block > 0 ? o.block : 4; }
 double now_s();

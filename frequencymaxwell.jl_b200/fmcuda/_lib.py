@@ -34,7 +34,7 @@ EXPORTED = (
     "fm_set_potential", "fm_green_apply", "fm_apply_operator", "fm_apply_preconditioner", "fm_curl_field",
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
     "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream", "fm_green_apply_noalloc",
-    "fm_engine_slot_bytes", "fm_engine_create", "fm_engine_destroy", "fm_engine_submit", "fm_engine_step",
+    "fm_engine_slot_bytes", "fm_engine_slot_bytes_ortho", "fm_engine_create", "fm_engine_destroy", "fm_engine_submit", "fm_engine_step",
     "fm_engine_status", "fm_plan_set_tuning", "fm_plan_get_tuning",
 )
 
@@ -118,6 +118,8 @@ def lib() -> C.CDLL:
     L.fm_plan_get_tuning.restype = C.c_int
     L.fm_engine_slot_bytes.argtypes = [C.POINTER(fm_plan_desc), C.c_int]
     L.fm_engine_slot_bytes.restype = C.c_longlong
+    L.fm_engine_slot_bytes_ortho.argtypes = [C.POINTER(fm_plan_desc), C.c_int, C.c_int]
+    L.fm_engine_slot_bytes_ortho.restype = C.c_longlong
     L.fm_engine_create.argtypes = [P, C.c_int, C.c_int, C.c_double, C.c_double, P, P, P, C.c_int, C.POINTER(P)]
     L.fm_engine_create.restype = C.c_int
     L.fm_engine_destroy.argtypes = [P]

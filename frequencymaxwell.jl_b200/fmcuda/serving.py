@@ -6,7 +6,9 @@ illuminations, a tolerance) of mixed grid shapes are served concurrently:
 * one engine per grid shape, its slot count sized from a device-memory budget split across the shapes;
 * a request's right-hand sides queue on their shape's engine and are admitted into slots as slots free
   up; every engine step advances all running right-hand sides by one GMRES iteration in shared launches
-  (continuous batching at iteration granularity);
+  (continuous batching at iteration granularity), or, with ``ortho="block"``, a right-hand side whose
+  iteration limit fits the basis by one s-step block of 8 iterations (block GMRES on FP64 block vectors, as
+  the batched solve runs it);
 * each shape's engine is stepped by its own host thread on its own CUDA stream, so shapes overlap on the
   device;
 * per-request latency (arrival to completion of its last right-hand side) and throughput are recorded.
@@ -32,7 +34,7 @@ from .medium import Medium, phantom_random_beads
 from .solver import ConvergentBornSolver, DevicePlan
 from .sources import PlaneWaveSource, illumination_cone
 
-_ORTHO = {"cgs": L.FM_ORTHO_CGS, "cgs2": L.FM_ORTHO_CGS2}
+_ORTHO = {"cgs": L.FM_ORTHO_CGS, "cgs2": L.FM_ORTHO_CGS2, "block": L.FM_ORTHO_BLOCK}
 
 
 @dataclass
@@ -62,9 +64,9 @@ class Request:
                                     resolution, self.sources[rhs].wavelength)
 
 
-def engine_slot_bytes(solver: ConvergentBornSolver, basis: int) -> int:
-    """Device bytes one slot of an engine on ``solver``'s grid holds (fm_engine_slot_bytes)."""
-    return int(L.lib().fm_engine_slot_bytes(C.byref(solver.plan().desc), int(basis)))
+def engine_slot_bytes(solver: ConvergentBornSolver, basis: int, ortho: str = "cgs") -> int:
+    """Device bytes one slot of an engine on ``solver``'s grid holds (fm_engine_slot_bytes_ortho)."""
+    return int(L.lib().fm_engine_slot_bytes_ortho(C.byref(solver.plan().desc), int(basis), _ORTHO[ortho]))
 
 
 class Engine:
@@ -86,8 +88,9 @@ class Engine:
         self._keep: Dict[int, tuple] = {}
         self._lock = threading.Lock()
 
-    def submit(self, req: Request):
-        """Queue every right-hand side of ``req``; results land in req.E / req.H (grid x 3 x nrhs)."""
+    def submit(self, req: Request, iterations_max: Optional[int] = None):
+        """Queue every right-hand side of ``req``; results land in req.E / req.H (grid x 3 x nrhs).
+        ``iterations_max`` overrides the solver's setting (Bornmax when >= 0) for this request."""
         g = self.grid
         eps = np.asfortranarray(req.medium.permittivity, dtype=np.complex128)
         n = len(req.sources)
@@ -105,8 +108,9 @@ class Engine:
         with self._lock:
             self._keep[req.req_id] = (req, eps, arr)
         req.submitted = time.perf_counter()
-        st = L.lib().fm_engine_submit(self.handle, req.req_id, L.ptr(eps), n, arr, req.tolerance,
-                                      self.solver.iterations_max, L.ptr(req.E), L.ptr(req.H))
+        itmax = self.solver.iterations_max if iterations_max is None else int(iterations_max)
+        st = L.lib().fm_engine_submit(self.handle, req.req_id, L.ptr(eps), n, arr, req.tolerance, itmax,
+                                      L.ptr(req.E), L.ptr(req.H))
         if st != L.FM_OK:
             with self._lock:
                 del self._keep[req.req_id]
@@ -166,7 +170,7 @@ def serving_boundaries(shape) -> tuple:
 
 
 def slot_plan(shapes: Sequence[Tuple[int, int, int]], budget_bytes: float, basis: int, precision: str,
-              resolution=(50e-9,) * 3, max_slots: int = 64, target_elements: float = 48e6
+              resolution=(50e-9,) * 3, max_slots: int = 64, target_elements: float = 48e6, ortho: str = "cgs"
               ) -> Dict[Tuple[int, int, int], int]:
     """Slots per shape under one device-memory budget.
 
@@ -184,7 +188,7 @@ def slot_plan(shapes: Sequence[Tuple[int, int, int]], budget_bytes: float, basis
         d.pad[:] = list(sv.padding())
         d.precision = {"float64": L.FM_PREC_F64, "float32": L.FM_PREC_F32,
                        "float32-math64": L.FM_PREC_F32_MATH64}[precision]
-        per[tuple(s)] = int(L.lib().fm_engine_slot_bytes(C.byref(d), int(basis)))
+        per[tuple(s)] = int(L.lib().fm_engine_slot_bytes_ortho(C.byref(d), int(basis), _ORTHO[ortho]))
         field = 3.0 * float(np.prod(sv.padded_size()))
         want[tuple(s)] = int(min(max_slots, max(1, np.ceil(target_elements / field))))
     base = sum(per.values())                     # one slot per shape first
@@ -202,7 +206,7 @@ class Server:
                  slots: Optional[Dict[Tuple[int, int, int], int]] = None, ortho: str = "cgs"):
         self.resolution = tuple(resolution)
         self.slots = dict(slots) if slots is not None else slot_plan(shapes, budget_bytes, basis, precision,
-                                                                     resolution, max_slots)
+                                                                     resolution, max_slots, ortho=ortho)
         self.engines: Dict[Tuple[int, int, int], Engine] = {}
         for shape in shapes:
             shape = tuple(shape)

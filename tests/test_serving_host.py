@@ -50,3 +50,19 @@ def test_request_stream_is_seeded_and_poisson():
         for s in r.sources:
             assert abs(np.linalg.norm(s.k_vector) - 1) < 1e-12
             assert abs(np.vdot(s.polarization, s.k_vector)) < 1e-12
+
+
+def test_block_engine_slot_bytes_include_block_vectors():
+    grid, basis = (32, 32, 16), 112
+    d = F._lib.fm_plan_desc()
+    d.grid[:] = list(grid)
+    d.pad[:] = [0, 0, grid[2] // 2]
+    d.precision = F._lib.FM_PREC_F32_MATH64
+    n = grid[0] * grid[1] * 2 * grid[2]
+    L = F._lib.lib()
+    cgs = L.fm_engine_slot_bytes_ortho(d, basis, F._lib.FM_ORTHO_CGS)
+    blk = L.fm_engine_slot_bytes_ortho(d, basis, F._lib.FM_ORTHO_BLOCK)
+    assert cgs == L.fm_engine_slot_bytes(d, basis)
+    assert blk - cgs >= 3 * n * 16 * 9  # 9 FP64 block vectors
+    plan = SV.slot_plan(SV.SERVING_SHAPES, 150e9, basis, "float32-math64", ortho="block")
+    assert all(v >= 1 for v in plan.values())
