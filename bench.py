@@ -425,17 +425,20 @@ def run(args):
 def run_serving(args):
     """Continuous batching of a seeded Poisson request stream (bounded sample of the serving workload):
     grids drawn uniformly from {64x64x32, 96x96x64, 128x128x64, 256x256x128}, 1-32 angles each, 12-bead
-    phantoms, complex64 fields with FP64 dots, tolerance 1e-5, slots sized from a 150 GB device budget."""
+    phantoms, complex64 fields with FP64 dots, tolerance 1e-5, slots sized from a 150 GB device budget.  With
+    the default ortho "block", right-hand sides whose iteration limit fits the basis run s-step block GMRES (one
+    block of 8 iterations per engine step), the others CGS GMRES(basis)."""
     from fmcuda import serving as SV
     reqs = SV.serving_requests(args.serving_requests, rate=args.serving_rate, seed=SEED)
     srv = SV.Server(SV.SERVING_SHAPES, budget_bytes=args.serving_budget_gb * 1e9, basis=args.serving_basis,
-                    precision=args.precision)
+                    precision=args.precision, ortho=args.serving_ortho)
     try:
         srv.start()
         rep = SV.run_stream(srv, reqs, timeout=1800)
     finally:
         srv.stop()
-    rep.update({"budget_GB": args.serving_budget_gb, "basis": args.serving_basis, "tolerance": 1e-5,
+    rep.update({"budget_GB": args.serving_budget_gb, "basis": args.serving_basis, "ortho": args.serving_ortho,
+                "tolerance": 1e-5,
                 "rate_req_per_s": args.serving_rate, "shapes": ["x".join(map(str, s)) for s in SV.SERVING_SHAPES],
                 "latency": "request arrival to its last right-hand side's fields on the host",
                 "iterations": {"min": min(i["iterations"] for r in reqs for i in r.infos.values()),
@@ -569,7 +572,9 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=8, help="requests in the serving sample (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
-    ap.add_argument("--serving-basis", type=int, default=100)
+    ap.add_argument("--serving-basis", type=int, default=112, help="Krylov basis per slot (block slots need "
+                    "maxiters + 8 <= basis)")
+    ap.add_argument("--serving-ortho", default="block", choices=["cgs", "cgs2", "block"])
     ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
     ap.add_argument("--large-only", action="store_true", help="run the large single configuration and print it")
     ap.add_argument("--large-check", type=int, default=1, help="with the large configuration: FP32 vs FP64 check at 128x128x256")

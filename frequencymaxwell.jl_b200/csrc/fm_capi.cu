@@ -209,7 +209,7 @@ void fm_plan_destroy(fm_plan* P) {
                     &P->wt_y, &P->wt_z, &P->wt_pe, &P->wt_ph, &P->wt_first, &P->Eo, &P->Ho, &P->errbuf,
                     &P->shifts, &P->yblk, &P->V64, &P->gtw[0], &P->gtw[1], &P->gtw[2], &P->gch[0][0],
                     &P->gch[0][1], &P->gch[1][0], &P->gch[1][1], &P->gch[2][0], &P->gch[2][1], &P->gkn[0][0],
-                    &P->gkn[0][1], &P->gkn[1][0], &P->gkn[1][1], &P->gkn[2][0], &P->gkn[2][1]};
+                    &P->gkn[0][1], &P->gkn[1][0], &P->gkn[1][1], &P->gkn[2][0], &P->gkn[2][1], &P->shapes};
   for (DevBuf* b : bufs) b->release();
   tk_resolve(P);
   for (cudaEvent_t e : P->evpool) cudaEventDestroy(e);
@@ -363,8 +363,11 @@ template <typename R>
 static fm_status build_potential_t(fm_plan* P, const double* eps, double eps_bg, double wl, const double* fx,
                                    const double* fy, const double* fz, int itmax, fm_potential_info* info) {
   const long long g = (long long)P->pi.gx * P->pi.gy * P->pi.gz;
-  FM_CK(P->eps_dev.ensure((size_t)g * sizeof(double2)));
-  FM_CK(cudaMemcpyAsync(P->eps_dev.p, eps, (size_t)g * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+  if (eps) {  // else the permittivity fm_phantom_fill painted on the device
+    FM_CK(P->eps_dev.ensure((size_t)g * sizeof(double2)));
+    FM_CK(cudaMemcpyAsync(P->eps_dev.p, eps, (size_t)g * sizeof(double2), cudaMemcpyHostToDevice, P->st));
+    P->eps_phantom = false;
+  }
   {
     // NaN/Inf in the permittivity would propagate silently (fmax ignores NaN): reject it here
     FM_CK(P->maxout.ensure(sizeof(double) + sizeof(unsigned) + sizeof(unsigned long long) + 8));
@@ -432,7 +435,7 @@ static fm_status build_potential_t(fm_plan* P, const double* eps, double eps_bg,
 fm_status fm_build_potential(fm_plan* P, const double* eps, double eps_bg, double wl, const double* fx, const double* fy,
                              const double* fz, int itmax, fm_potential_info* info) {
   FM_TRY(check_plan(P, 1, false));
-  if (!eps) return fail(FM_ERR_INVALID, "null permittivity");
+  if (!eps && !P->eps_phantom) return fail(FM_ERR_INVALID, "null permittivity and no device phantom (fm_phantom_fill)");
   if (!(eps_bg > 0)) return fail(FM_ERR_INVALID, "permittivity_bg must be positive");
   if (!(wl > 0)) return fail(FM_ERR_INVALID, "wavelength must be positive");
   return P->prec == FM_PREC_F64 ? build_potential_t<double>(P, eps, eps_bg, wl, fx, fy, fz, itmax, info)

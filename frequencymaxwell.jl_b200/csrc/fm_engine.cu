@@ -171,7 +171,7 @@ fm_status fm_engine_create(fm_plan* P, int slots, int basis, double wavelength, 
   al(E->maxo, 64);
   // block slots: block vectors, pass temporaries and potentials of the block-vector type (FP64 unless the plan
   // computes in FP32), per-slot index arrays, update coefficients of a whole block
-  const size_t ysz = P->prec == FM_PREC_F32 ? esz : sizeof(double2), tsz = E->bs ? std::max(esz, ysz) : esz;
+  const size_t ysz = P->c64 ? sizeof(double2) : esz, tsz = E->bs ? std::max(esz, ysz) : esz;
   if (E->bs) {
     al(E->Yb, (size_t)(E->bs + 1) * S * M * ysz);
     if (ysz != esz) al(E->V64s, S * n * ysz);
@@ -454,11 +454,14 @@ static fm_status engine_step_t(fm_engine* E) {
       sl.eps_imag = std::max(std::pow(2.0, -20), vmax * 1.01);
       ksqh[s] = sl.eps_imag / kref2;
       iepsh[s] = kref2 / sl.eps_imag;
+      const bool v64 = E->bs && sizeof(TY) != sizeof(T);
+      if (E->Vs.cap < (size_t)(s + 1) * n * sizeof(T) || (v64 && E->V64s.cap < (size_t)(s + 1) * n * sizeof(double2)))
+        return fail(FM_ERR_INVALID, "engine potential buffers smaller than the slots");
       k_potential_build<R><<<1184, 256, 0, P->st>>>(P->pi, (const double2*)E->epsd.p, E->eps_bg, k2, sl.eps_imag,
                                                     (const double*)P->fx.p, (const double*)P->fy.p,
                                                     (const double*)P->fz.p, 1.0 / kref2, (T*)E->Vs.p + (size_t)s * n);
       FM_CK(cudaGetLastError());
-      if (E->bs && sizeof(TY) != sizeof(T)) {  // the block vectors' operator reads an FP64 potential
+      if (v64) {  // the block vectors' operator reads the same potential widened to FP64
         k_to_f64<R><<<2 * P->sms, 256, 0, P->st>>>((long long)n, (const T*)E->Vs.p + (size_t)s * n, 1.0,
                                                    (double2*)E->V64s.p + (size_t)s * n);
         FM_CK(cudaGetLastError());

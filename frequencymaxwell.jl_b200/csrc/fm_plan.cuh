@@ -106,6 +106,8 @@ struct fm_plan {
   DevBuf t1, t2, t3, bbuf, xbuf, ebuf, sbuf, basis, gbuf2;  // t3: first branch of a two-branch average
   DevBuf red_part, red_out, red_cnt, active, scale, coef, hbuf, shifts, yblk, V64;
   DevBuf eps_dev, fx, fy, fz, maxpart, maxout;
+  bool eps_phantom = false;  // eps_dev holds the permittivity fm_phantom_fill painted (fm_build_potential eps = NULL)
+  DevBuf shapes;             // fm_phantom_fill's shape table
   DevBuf wt_x, wt_y, wt_z, wt_pe, wt_ph, wt_first;
   DevBuf Eo, Ho;
   int out_nrhs = 0;

@@ -8,8 +8,8 @@ from .boundary import (AbsorbingBoundaryCondition, AbstractBoundaryCondition, At
                        create_attenuation_window, padding_pixels, requires_averaging, requires_padding,
                        subpixel_shift)
 from .fields import ElectromagneticField, crop_to_ROI, field_energy, field_intensity, to_host
-from .medium import (AbstractMedium, Medium, grid_size, permittivity, permittivity_bg, phantom_bead,
-                     phantom_cylinder, phantom_plate, phantom_random_beads)
+from .medium import (AbstractMedium, DevicePhantom, Medium, Shape, grid_size, paint_host, permittivity,
+                     permittivity_bg, phantom_bead, phantom_cylinder, phantom_plate, phantom_random_beads)
 from .solver import (BornSeries, ConvergentBornSolver, DevicePlan, KrylovJL_BICGSTAB, KrylovJL_GMRES, compute_ROI,
                      domain_size, grid_spacing, reset, solve, solve_batch)
 from .sources import (AbstractCurrentSource, PlaneWaveSource, generate_incident_field, illumination_cone,

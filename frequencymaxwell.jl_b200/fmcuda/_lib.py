@@ -21,6 +21,7 @@ FM_ORTHO_MGS, FM_ORTHO_CGS, FM_ORTHO_CGS2, FM_ORTHO_BLOCK = 0, 1, 2, 3
 FM_BLOCK_FP64, FM_BLOCK_STORAGE, FM_BLOCK_FP64_ORTHO = 0, 1, 2
 FM_TUNE_Y_TMA, FM_TUNE_Z_TMA, FM_TUNE_TMA_CTAS_PER_SM, FM_TUNE_ROW_THREADS, FM_TUNE_WAVE_RHS = 0, 1, 2, 3, 4
 FM_TUNE_BLOCK_DOT = 5
+FM_SHAPE_SPHERE, FM_SHAPE_PLATE, FM_SHAPE_CYLINDER = 0, 1, 2
 
 STATUS_NAMES = {
     FM_OK: "FM_OK", FM_ERR_INVALID: "FM_ERR_INVALID", FM_ERR_OOM: "FM_ERR_OOM",
@@ -35,7 +36,7 @@ EXPORTED = (
     "fm_solve_source", "fm_build_potential", "fm_solve_plane_waves", "fm_copy_fields", "fm_synchronize",
     "fm_set_profiling", "fm_kernel_stats", "fm_launch_count", "fm_stream", "fm_green_apply_noalloc",
     "fm_engine_slot_bytes", "fm_engine_slot_bytes_ortho", "fm_engine_create", "fm_engine_destroy", "fm_engine_submit", "fm_engine_step",
-    "fm_engine_status", "fm_plan_set_tuning", "fm_plan_get_tuning",
+    "fm_engine_status", "fm_plan_set_tuning", "fm_plan_get_tuning", "fm_phantom_fill",
 )
 
 
@@ -62,6 +63,11 @@ class fm_potential_info(C.Structure):
 class fm_plane_wave(C.Structure):
     _fields_ = [("wavelength", C.c_double), ("polarization", C.c_double * 6), ("k_vector", C.c_double * 3),
                 ("amplitude", C.c_double), ("phase", C.c_double)]
+
+
+class fm_shape(C.Structure):
+    _fields_ = [("kind", C.c_int), ("axis", C.c_int), ("center", C.c_double * 3), ("radius", C.c_double),
+                ("extent", C.c_double), ("value", C.c_double * 2)]
 
 
 class fm_kernel_stat(C.Structure):
@@ -133,6 +139,8 @@ def lib() -> C.CDLL:
     L.fm_engine_status.restype = C.c_int
     L.fm_green_apply_noalloc.argtypes = [C.POINTER(fm_plan_desc), C.c_double, C.c_double, C.c_int, P, P, P]
     L.fm_green_apply_noalloc.restype = C.c_int
+    L.fm_phantom_fill.argtypes = [P, C.c_double, C.c_int, C.POINTER(fm_shape), P]
+    L.fm_phantom_fill.restype = C.c_int
     L.fm_stream.argtypes = [P]
     L.fm_stream.restype = C.c_void_p
     for name in ("fm_plan_create", "fm_set_potential", "fm_green_apply", "fm_apply_operator",

@@ -23,7 +23,7 @@ from . import _lib as L
 from .boundary import (AbsorbingBoundaryCondition, AbstractBoundaryCondition, PeriodicBoundaryCondition,
                        attenuation_filter, padding_pixels, requires_averaging, requires_padding, subpixel_shift)
 from .fields import ElectromagneticField
-from .medium import Medium, grid_size as medium_grid_size
+from .medium import DevicePhantom, Medium, grid_size as medium_grid_size
 from .sources import PlaneWaveSource, as_list, source_wavelength
 
 
@@ -249,15 +249,35 @@ class DevicePlan:
             raise ValueError("potential must have the padded grid shape")
         L.check(L.lib().fm_set_potential(self.handle, L.ptr(V), k_bg, eps_imag, wavelength))
 
-    def build_potential(self, eps: np.ndarray, eps_bg: float, wavelength: float, filters, iterations_max: int):
-        eps = np.asfortranarray(np.asarray(eps, dtype=np.complex128))
-        if eps.shape != self.grid:
-            raise ValueError(f"medium grid_size {eps.shape} must match solver grid_size {self.grid}")
+    def build_potential(self, eps: Optional[np.ndarray], eps_bg: float, wavelength: float, filters,
+                        iterations_max: int):
+        """_initialize_solver! on the device; eps None takes the permittivity fill_phantom painted there."""
+        if eps is not None:
+            eps = np.asfortranarray(np.asarray(eps, dtype=np.complex128))
+            if eps.shape != self.grid:
+                raise ValueError(f"medium grid_size {eps.shape} must match solver grid_size {self.grid}")
         info = L.fm_potential_info()
         fx, fy, fz = (np.ascontiguousarray(f, dtype=np.float64) for f in filters)
-        L.check(L.lib().fm_build_potential(self.handle, L.ptr(eps), eps_bg, wavelength, L.ptr(fx), L.ptr(fy),
-                                           L.ptr(fz), int(iterations_max), C.byref(info)))
+        L.check(L.lib().fm_build_potential(self.handle, None if eps is None else L.ptr(eps), eps_bg, wavelength,
+                                           L.ptr(fx), L.ptr(fy), L.ptr(fz), int(iterations_max), C.byref(info)))
         return info
+
+    def fill_phantom(self, shapes, eps_bg: float, copy_out: bool = False) -> Optional[np.ndarray]:
+        """Paint ``shapes`` (medium.Shape, in order) over eps_bg into the plan's device permittivity."""
+        arr = (L.fm_shape * max(1, len(shapes)))()
+        for i, sh in enumerate(shapes):
+            arr[i].kind = int(sh.kind)
+            arr[i].axis = int(sh.axis)
+            for a in range(3):
+                arr[i].center[a] = float(sh.center[a])
+            arr[i].radius = float(sh.radius)
+            arr[i].extent = float(sh.extent)
+            arr[i].value[0] = complex(sh.value).real
+            arr[i].value[1] = complex(sh.value).imag
+        out = np.empty(self.grid, dtype=np.complex128, order="F") if copy_out else None
+        L.check(L.lib().fm_phantom_fill(self.handle, float(eps_bg), len(shapes), arr,
+                                        None if out is None else L.ptr(out)))
+        return out
 
     def green_apply(self, x: np.ndarray) -> np.ndarray:
         x = self._field(x)
@@ -358,8 +378,13 @@ def _prepare(solver: ConvergentBornSolver, medium: Medium, wavelength: float):
         raise ValueError(f"medium grid_size {medium_grid_size(medium)} must match solver grid_size "
                          f"{solver.grid_size}")
     plan = solver.plan()
-    info = plan.build_potential(medium.permittivity, medium.permittivity_bg, wavelength,
-                                solver.attenuation_filters(), solver.iterations_max)
+    eps = None
+    if isinstance(medium, DevicePhantom):  # painted on the device: no permittivity crosses from the host
+        plan.fill_phantom(medium.shapes, medium.permittivity_bg)
+    else:
+        eps = medium.permittivity
+    info = plan.build_potential(eps, medium.permittivity_bg, wavelength, solver.attenuation_filters(),
+                                solver.iterations_max)
     solver.Bornmax = int(info.bornmax)
     solver.iteration_count = 0
     solver.residual_history.clear()

@@ -155,9 +155,32 @@ fm_status fm_solve_source(fm_plan* plan, int nrhs, const double* S, const fm_sol
  * device from the unpadded permittivity (Nx, Ny, Nz) complex array.  fx, fy, fz
  * are the per-axis attenuation filters over the padded axes (all ones on
  * periodic axes), as _apply_attenuation_to_potential! builds them
- * (convergent_born.jl:893-944). */
+ * (convergent_born.jl:893-944).  eps = NULL takes the permittivity that fm_phantom_fill painted on the
+ * device. */
 fm_status fm_build_potential(fm_plan* plan, const double* eps, double eps_bg, double wavelength, const double* fx,
                              const double* fy, const double* fz, int iterations_max, fm_potential_info* info);
+
+/* ---- phantoms painted on the device (phantoms.jl:58-362) ----
+ * The reference's phantom generators fill a host array: the background, then spheres (_fill_sphere!,
+ * phantoms.jl:212-247: bounding box [max(1, round(c - r)), min(N, round(c + r))] per axis, then
+ * (i-c1)^2 + (j-c2)^2 + (k-c3)^2 <= r^2 with 1-based indices), plates (phantom_plate, :156-199: the slab
+ * [max(1, round(c - t/2)), min(N, round(c + t/2))] along its normal) and cylinders (phantom_cylinder /
+ * _fill_cylinder!, :272-362: that range along the axis, and the squared distance over the two other axes
+ * <= r^2).  fm_phantom_fill paints the same shapes, in order (later shapes overwrite earlier ones), into the
+ * plan's device permittivity (grid_size, complex FP64) with the same FP64 tests, bit for bit; the next
+ * fm_build_potential with eps = NULL builds the potential from it, so no permittivity crosses from the host.
+ * eps_out (optional, host, (Nx, Ny, Nz) complex FP64) receives a copy.  `round` is to nearest, ties to even. */
+enum { FM_SHAPE_SPHERE = 0, FM_SHAPE_PLATE = 1, FM_SHAPE_CYLINDER = 2 };
+typedef struct {
+  int kind;             /* FM_SHAPE_* */
+  int axis;             /* plate normal / cylinder axis, 1..3 (spheres: unused) */
+  double center[3];     /* 1-based voxel coordinates; (N+1)/2 is the grid centre as in the reference */
+  double radius;        /* sphere / cylinder radius in pixels */
+  double extent;        /* plate thickness / cylinder height in pixels */
+  double value[2];      /* permittivity (re, im) */
+} fm_shape;
+fm_status fm_phantom_fill(fm_plan* plan, double permittivity_bg, int nshapes, const fm_shape* shapes,
+                          double* eps_out);
 
 /* The whole of solve(solver, sources, medium) after set-up (convergent_born.jl:576-599):
  * incident plane waves (generate_incident_field, plane_wave.jl:198-268, coherent sum

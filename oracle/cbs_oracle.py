@@ -902,6 +902,37 @@ def phantom_plate(grid_size, permittivity_profile, thickness_pixel: float, permi
     return ph
 
 
+def fill_cylinder(ph: np.ndarray, center, radius: float, axis_start: int, axis_end: int, axis: int,
+                  value: complex) -> None:
+    """_fill_cylinder! (phantoms.jl:315-362): along `axis` (1..3) from axis_start to axis_end (1-based,
+    inclusive), the voxels whose squared distance over the two other axes (in increasing axis order) is <= r^2."""
+    g = ph.shape
+    r2 = radius ** 2
+    a = axis - 1
+    o = [d for d in range(3) if d != a]
+    u = np.arange(1, g[o[0]] + 1).reshape(-1, 1) - center[o[0]]
+    v = np.arange(1, g[o[1]] + 1).reshape(1, -1) - center[o[1]]
+    disk = u * u + v * v <= r2
+    for idx in range(axis_start - 1, axis_end):
+        sl = [slice(None)] * 3
+        sl[a] = idx
+        ph[tuple(sl)][disk] = value
+
+
+def phantom_cylinder(grid_size, permittivity_profile, radius_pixel: float, permittivity_bg: float = 1.0,
+                     height_pixel: Optional[float] = None, axis: int = 3) -> np.ndarray:
+    """phantom_cylinder (phantoms.jl:272-313): a cylinder about the grid centre (N+1)/2 along `axis`, extent
+    [max(1, round(c - h/2)), min(N, round(c + h/2))]."""
+    if height_pixel is None:
+        height_pixel = 2 * radius_pixel
+    ph = np.full(tuple(grid_size), complex(permittivity_bg), dtype=np.complex128, order="F")
+    c = [(grid_size[d] + 1) / 2 for d in range(3)]
+    s = max(1, julia_round(c[axis - 1] - height_pixel / 2))
+    e = min(grid_size[axis - 1], julia_round(c[axis - 1] + height_pixel / 2))
+    fill_cylinder(ph, c, radius_pixel, s, e, axis, complex(permittivity_profile[0]))
+    return ph
+
+
 # ----------------------------------------------------------------------------
 # solve  (convergent_born.jl:565-600, 703-774)
 # ----------------------------------------------------------------------------

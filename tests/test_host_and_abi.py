@@ -96,9 +96,30 @@ def test_phantoms_match_oracle():
                                       O.phantom_bead(g, eps, r, permittivity_bg=1.7))
     np.testing.assert_array_equal(F.phantom_plate((21, 50, 50), [2.0], 4, permittivity_bg=1.0).permittivity,
                                   O.phantom_plate((21, 50, 50), [2.0], 4, permittivity_bg=1.0))
+    for ax in (1, 2, 3):
+        np.testing.assert_array_equal(
+            F.phantom_cylinder((21, 30, 17), [2.0 + 0.1j], 5.5, permittivity_bg=1.3, height_pixel=7, axis=ax).permittivity,
+            O.phantom_cylinder((21, 30, 17), [2.0 + 0.1j], 5.5, permittivity_bg=1.3, height_pixel=7, axis=ax))
     m = F.phantom_random_beads((64, 64, 32), 6, (2, 6), (1.36, 1.6), 1.33 ** 2, 3)
     assert m.permittivity.shape == (64, 64, 32)
     assert np.all(m.permittivity.real >= 1.33 ** 2 - 1e-12)
+
+
+def test_device_phantom_shapes_paint_like_the_host_generators():
+    """on_device=True returns the shape list; painting it on the host gives the generator's array."""
+    cases = [lambda d: F.phantom_bead((21, 22, 23), [2.0, 3.0], 4.5, permittivity_bg=1.7, on_device=d),
+             lambda d: F.phantom_plate((21, 50, 50), [2.0], 4, permittivity_bg=1.0, plate_normal=2, on_device=d),
+             lambda d: F.phantom_cylinder((21, 30, 17), [2.0], 5.5, permittivity_bg=1.3, axis=1, on_device=d),
+             lambda d: F.phantom_random_beads((64, 64, 32), 6, (2, 6), (1.36, 1.6), 1.33 ** 2, 3, on_device=d)]
+    for make in cases:
+        host, dev = make(False), make(True)
+        assert isinstance(dev, F.DevicePhantom) and F.grid_size(dev) == host.permittivity.shape
+        np.testing.assert_array_equal(dev.permittivity, host.permittivity)
+    # later shapes overwrite earlier ones; bounding boxes round half to even (round(2.5) = 2)
+    sh = [F.Shape(0, (4.5, 4.5, 4.5), 2.0, radius=2.0), F.Shape(1, (0, 0, 4.5), 3.0, axis=3, extent=1.0),
+          F.Shape(2, (4.5, 4.5, 4.5), 4.0, radius=1.0, axis=1, extent=3.0)]
+    ph = F.paint_host((8, 8, 8), sh, 1.0)
+    assert ph[3, 3, 3] == 4.0 and ph[0, 0, 3] == 3.0 and ph[0, 0, 4] == 3.0 and ph[0, 0, 5] == 1.0
 
 
 def test_incident_field_matches_oracle():
