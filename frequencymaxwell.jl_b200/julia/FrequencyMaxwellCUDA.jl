@@ -80,6 +80,49 @@ struct FMPlaneWave
     phase::Cdouble
 end
 
+# fm_shape: one region of a phantom painted on the device (fm_phantom_fill)
+const FM_SHAPE_SPHERE, FM_SHAPE_PLATE, FM_SHAPE_CYLINDER = Cint(0), Cint(1), Cint(2)
+struct FMShape
+    kind::Cint
+    axis::Cint
+    center::NTuple{3,Cdouble}
+    radius::Cdouble
+    extent::Cdouble
+    value::NTuple{2,Cdouble}
+end
+
+# phantom_bead's spheres (phantoms.jl:84-100): beads stacked along z about the grid centre (N+1)/2
+function bead_shapes(grid_size::NTuple{3,Int}, permittivity_profile, pixel_radius::Real;
+                     bead_distance::Real = 2 * pixel_radius)
+    n = length(permittivity_profile)
+    c = ntuple(i -> (grid_size[i] + 1) / 2, 3)
+    shapes = FMShape[]
+    for b in 1:n
+        zc = c[3] + (b - (n + 1) / 2) * bead_distance
+        (zc < 1 || zc > grid_size[3]) && continue
+        v = ComplexF64(permittivity_profile[(b - 1) % n + 1])
+        push!(shapes, FMShape(FM_SHAPE_SPHERE, Cint(3), (c[1], c[2], zc), pixel_radius, 0.0, (real(v), imag(v))))
+    end
+    return shapes
+end
+
+# paint `shapes` (in order) over permittivity_bg into the plan's device permittivity; the next
+# build_potential_device! builds the potential from it without a host array
+function phantom_fill!(plan, permittivity_bg::Real, shapes::Vector{FMShape})
+    check(ccall((:fm_phantom_fill, libfmcuda), Cint, (Ptr{Cvoid}, Cdouble, Cint, Ptr{FMShape}, Ptr{ComplexF64}),
+                plan, permittivity_bg, length(shapes), shapes, C_NULL))
+end
+
+function build_potential_device!(plan, solver, permittivity_bg::Real, wavelength)
+    fx, fy, fz = (attenuation_filter(solver, d) for d in 1:3)
+    pinfo = Ref{FMPotentialInfo}()
+    check(ccall((:fm_build_potential, libfmcuda), Cint,
+                (Ptr{Cvoid}, Ptr{ComplexF64}, Cdouble, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Cint,
+                 Ref{FMPotentialInfo}),
+                plan, C_NULL, permittivity_bg, wavelength, fx, fy, fz, solver.iterations_max, pinfo))
+    return Int(pinfo[].bornmax)
+end
+
 function check(status)
     status == FM_OK && return status
     msg = unsafe_string(ccall((:fm_last_error, libfmcuda), Cstring, ()))
