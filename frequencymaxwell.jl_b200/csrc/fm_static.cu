@@ -9,8 +9,8 @@
 // Scratch: one file-scope __device__ array of FM_NOALLOC_SCRATCH_BYTES (64 MiB) holds the twiddle and
 // ramp tables, the error flag of the pipelined passes and one field-sized temporary.  Every GPU that
 // loads the library keeps it until the process exits.  Its device address is looked up once per device
-// (cudaGetSymbolAddress with that device current) on the first call that uses the device; make that
-// first call before any stream capture.  All calls share the array and it keeps the last call's
+// (cudaGetSymbolAddress with that device current) on the first call that uses the device.  All calls
+// share the array and it keeps the last call's
 // contents, so calls that overlap on the GPU (different streams or threads) race; the error flag is
 // cleared at the start of every call.  Sizes whose temporary and tables do not fit are rejected with
 // FM_ERR_INVALID.  The output buffer doubles as the second pass temporary, so x and y must not overlap.

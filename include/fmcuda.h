@@ -239,8 +239,8 @@ fm_status fm_engine_status(fm_engine* engine, int* running, int* queued);
  * temporary).  desc gives grid, padding, resolution, boundaries, precision and device; max_rhs is
  * ignored.  The only scratch is one static 64 MiB device array per GPU that loads the library
  * (tables, an error flag and one field-sized temporary), so sizes whose temporary does not fit are
- * rejected with FM_ERR_INVALID.  The first call on a device looks up that array's address and should
- * come before any stream capture.  Calls share the array: calls that overlap on the GPU race.  Work is
+ * rejected with FM_ERR_INVALID.  The first call on a device looks up that array's address.  Calls share
+ * the array: calls that overlap on the GPU race.  Work is
  * issued on `stream` (NULL: default stream) and the call returns after it has finished. */
 fm_status fm_green_apply_noalloc(const fm_plan_desc* desc, double k_bg, double eps_imag, int nrhs, const void* x_dev,
                                  void* y_dev, void* stream);
