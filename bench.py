@@ -426,8 +426,8 @@ def run_serving(args):
     """Continuous batching of a seeded Poisson request stream (bounded sample of the serving workload):
     grids drawn uniformly from {64x64x32, 96x96x64, 128x128x64, 256x256x128}, 1-32 angles each, 12-bead
     phantoms, complex64 fields with FP64 dots, tolerance 1e-5, slots sized from a 150 GB device budget.  With
-    the default ortho "block", right-hand sides whose iteration limit fits the basis run s-step block GMRES (one
-    block of 8 iterations per engine step), the others CGS GMRES(basis)."""
+    the default ortho "block", the slots run s-step block GMRES (one block of 8 iterations per engine step),
+    restarted every basis iterations when their limit exceeds the basis."""
     from fmcuda import serving as SV
     reqs = SV.serving_requests(args.serving_requests, rate=args.serving_rate, seed=SEED)
     srv = SV.Server(SV.SERVING_SHAPES, budget_bytes=args.serving_budget_gb * 1e9, basis=args.serving_basis,

@@ -170,6 +170,13 @@ bool blk_init(BlkState& r, int ld, double beta, double abstol, double reltol) {
   return false;
 }
 
+void blk_restart(BlkState& r, int ld, double beta, double eps) {
+  blk_init(r, ld, beta, 0.0, 0.0);
+  r.active = true;
+  r.solved = false;
+  r.eps = eps;
+}
+
 bool blk_givens_col(BlkState& r, int j, int itmax) {
   const int ld = r.ld;
   const int K = j + 1;

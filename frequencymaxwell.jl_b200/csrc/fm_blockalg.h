@@ -39,6 +39,9 @@ void rf_solve_h(const BlkState& st, int K, const cdb* c, cdb* d);
 // Start of a solve from ||r0|| = beta: X_0 = r0, Rf = [beta].  Returns true when the right-hand side is solved
 // already (beta = 0 or beta <= abstol + reltol beta); it is then marked inactive.
 bool blk_init(BlkState& r, int ld, double beta, double abstol, double reltol);
+// A new cycle of restarted block GMRES from the updated residual ||r|| = beta, keeping the first cycle's
+// tolerance eps; as a restarted GMRES cycle begins, there is no stopping test here.
+void blk_restart(BlkState& r, int ld, double beta, double eps);
 // Givens update with Hessenberg column j (Krylov.jl gmres); true when the right-hand side stops at this column
 // (solved, Krylov breakdown, or itmax columns).
 bool blk_givens_col(BlkState& r, int j, int itmax);

@@ -23,13 +23,15 @@
 // result does not depend on the other slots.  All requests of an engine share
 // wavelength and background permittivity.
 //
-// With FM_ORTHO_BLOCK a slot whose iteration limit fits the basis (maxiters +
-// s + 1 stored vectors) runs the batched s-step block GMRES instead (s = 8, FP64
-// block vectors stored orthonormalised): its first s iterations share step 3's
-// CGS launches, after which each engine step advances it by one block of s
-// iterations (3b), in launches shared by every slot in that phase, each at its
-// own basis size.  The per-RHS algebra is that of the batched block solve
-// (fm_blockalg.cu).  Slots whose limit does not fit run CGS GMRES(basis).
+// With FM_ORTHO_BLOCK every slot runs s-step block GMRES (s = 8, FP64 block
+// vectors stored orthonormalised, the per-RHS algebra of the batched block solve,
+// fm_blockalg.cu): the first s iterations of a cycle share step 3's CGS launches,
+// after which each engine step advances the slot by one block of s iterations
+// (3b), in launches shared by every slot in that phase, each at its own basis
+// size.  A slot whose limit fits the basis (maxiters + s + 1 stored vectors) runs
+// full GMRES as the batched block solve does; otherwise it restarts when the
+// basis is full, every floor(basis / s) * s iterations (s-step GMRES(m), the
+// restart points of CGS GMRES(basis) when s divides the basis).
 // ===========================================================================
 struct EngineUnit {  // one queued right-hand side
   long long req;
@@ -48,8 +50,9 @@ struct EngineSlot {
   int state = SL_FREE;
   bool fresh = false;  // admitted, residual not formed yet
   bool blk = false;    // s-step block GMRES (FM_ORTHO_BLOCK engines, limit fits the basis)
-  int phase = 0;       // block slots: 1 = the first s CGS steps, 2 = blocks
-  int m = 0;           // block slots: Hessenberg columns done
+  int phase = 0;       // block slots: 1 = the first s CGS steps of a cycle, 2 = blocks
+  int m = 0;           // block slots: Hessenberg columns done in this cycle
+  int itbase = 0;      // block slots: iterations of the cycles before this one
   BlkState bst;
   EngineUnit u;
   int j = 0, inner = 0, iters = 0, maxiters = 100;
@@ -362,12 +365,16 @@ static fm_status engine_block_step(fm_engine* E, std::vector<int>& acth, const R
   for (int s : run) {
     EngineSlot& sl = E->slots[s];
     const bool stop = blk_absorb(sl.bst, sl.m, bs, true, Gt.data() + (size_t)s * NG, Cv[s],
-                                 rbi.data() + (size_t)s * bs * bs, sl.maxiters);
-    sl.iters = sl.bst.iters;
+                                 rbi.data() + (size_t)s * bs * bs, sl.maxiters - sl.itbase);
+    sl.iters = sl.itbase + sl.bst.iters;
     sl.rnorm = sl.bst.rnorm;
     sl.solved = sl.bst.solved;
-    if (stop) sl.state = SL_STOP;
-    else sl.m += bs;
+    if (stop) {
+      sl.state = SL_STOP;
+    } else {
+      sl.m += bs;
+      if (sl.m + bs > E->mem) sl.state = SL_RESTART;  // the next block would not fit: end the cycle
+    }
   }
   // V = Y' Rb^{-1} into each slot's basis rows m+1 .. m+s (also for slots that stopped in this block: their
   // solution uses these vectors; a block that lost rank gets zero coefficients and is not used)
@@ -468,7 +475,7 @@ static fm_status engine_step_t(fm_engine* E) {
       }
       // iteration limit of this right-hand side (convergent_born.jl:746)
       sl.maxiters = std::max(2 * engine_bornmax(P, sl.eps_imag, sl.u.itmax_setting), 100);
-      sl.blk = E->bs > 0 && sl.maxiters + E->bs + 1 <= E->mem + 1 && (M & 3) == 0;
+      sl.blk = E->bs > 0 && E->mem >= 2 * E->bs && (M & 3) == 0;
       FM_TRY(wave_tables(P, sl.u.src, E->eps_bg, tx.data(), ty.data(), tz.data(), pe.data(), ph.data()));
       FM_CK(cudaMemcpyAsync((double2*)E->wt_x.p + (size_t)s * n3[0], tx.data(), n3[0] * sizeof(double2),
                             cudaMemcpyHostToDevice, P->st));
@@ -520,6 +527,7 @@ static fm_status engine_step_t(fm_engine* E) {
           if (sl.blk) {
             sl.m = sl.j = 0;
             sl.phase = 1;
+            sl.itbase = 0;
             if (blk_init(sl.bst, E->mem + 2, sl.beta, sl.u.tol * 1e-2, sl.u.tol)) {
               sl.solved = true;
               sl.state = SL_STOP;
@@ -534,6 +542,11 @@ static fm_status engine_step_t(fm_engine* E) {
           sl.solved = true;
           sl.state = SL_STOP;
           continue;
+        } else if (sl.blk) {  // the next cycle of a block slot: a new basis from the updated residual
+          sl.itbase = sl.iters;
+          blk_restart(sl.bst, E->mem + 2, sl.beta, sl.eps);
+          sl.m = sl.j = 0;
+          sl.phase = 1;
         }
         E->sch[(size_t)0 * S + s] = 1.0 / sl.beta;
         sl.state = SL_RUN;
@@ -623,8 +636,8 @@ static fm_status engine_step_t(fm_engine* E) {
         if (sl.blk) {  // Hessenberg column m of the block solve, its Givens update and stop test
           BlkState& r = sl.bst;
           for (int i = 0; i < K; ++i) r.H[i + (size_t)sl.m * r.ld] = col[i];
-          const bool stop = blk_cgs_close(r, sl.m, hb, sl.maxiters);
-          sl.iters = r.iters;
+          const bool stop = blk_cgs_close(r, sl.m, hb, sl.maxiters - sl.itbase);
+          sl.iters = sl.itbase + r.iters;
           sl.rnorm = r.rnorm;
           sl.solved = r.solved;
           if (stop) {

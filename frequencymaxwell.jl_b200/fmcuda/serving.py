@@ -6,9 +6,9 @@ illuminations, a tolerance) of mixed grid shapes are served concurrently:
 * one engine per grid shape, its slot count sized from a device-memory budget split across the shapes;
 * a request's right-hand sides queue on their shape's engine and are admitted into slots as slots free
   up; every engine step advances all running right-hand sides by one GMRES iteration in shared launches
-  (continuous batching at iteration granularity), or, with ``ortho="block"``, a right-hand side whose
-  iteration limit fits the basis by one s-step block of 8 iterations (block GMRES on FP64 block vectors, as
-  the batched solve runs it);
+  (continuous batching at iteration granularity), or, with ``ortho="block"``, by one s-step block of 8
+  iterations (block GMRES on FP64 block vectors, as the batched solve runs it; restarted when the basis is
+  full);
 * each shape's engine is stepped by its own host thread on its own CUDA stream, so shapes overlap on the
   device;
 * per-request latency (arrival to completion of its last right-hand side) and throughput are recorded.

@@ -206,11 +206,12 @@ fm_status fm_synchronize(fm_plan* plan);
  * tolerance, abstol = tolerance*1e-2; when maxiters exceeds `basis` the slot restarts GMRES every `basis`
  * iterations, i.e. it runs GMRES(basis), and full GMRES as the reference when maxiters fits the basis).  Requests share the engine's
  * wavelength, background permittivity and attenuation filters (fx, fy, fz over the padded axes, NULL =
- * ones) and take over the plan.  ortho: FM_ORTHO_CGS, FM_ORTHO_CGS2, or FM_ORTHO_BLOCK, with which a slot
- * with maxiters + 8 <= basis (and 3 x padded voxels a multiple of 4) runs s-step block GMRES (s = 8, FP64 block vectors stored orthonormalised,
- * as fm_solve with FM_ORTHO_BLOCK and FM_BLOCK_FP64_ORTHO) and the other slots CGS.  fm_engine_step admits queued
- * right-hand sides into free slots, runs one Krylov iteration (a block slot: one block of 8 after its first 8
- * iterations) on every running slot in shared launches (slots at different iterations), and
+ * ones) and take over the plan.  ortho: FM_ORTHO_CGS, FM_ORTHO_CGS2, or FM_ORTHO_BLOCK, with which the slots
+ * run s-step block GMRES (s = 8, FP64 block vectors stored orthonormalised, as fm_solve with FM_ORTHO_BLOCK and
+ * FM_BLOCK_FP64_ORTHO; needs basis >= 16 and 3 x padded voxels a multiple of 4, else CGS): full GMRES when
+ * maxiters + 8 <= basis, otherwise restarted every floor(basis / 8) * 8 iterations.  fm_engine_step admits queued
+ * right-hand sides into free slots, runs one Krylov iteration (a block slot: one block of 8 after the first 8
+ * iterations of a cycle) on every running slot in shared launches (slots at different iterations), and
  * finishes the slots that stopped: their cropped total E and H are copied to the caller's host buffers
  * given at submission (nrhs x (Nx,Ny,Nz,3) complex FP64 each), which must stay valid until then.
  * fm_engine_submit may be called from another thread than fm_engine_step. */

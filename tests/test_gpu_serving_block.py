@@ -5,8 +5,9 @@ stored orthonormalised): its first 8 iterations share the engine's CGS launches,
 advances it by one block, in launches shared with the other block slots, each at its own basis size.  So:
 * a request alone in a block engine matches ``solve_batch`` with ``ortho="block"`` (same iteration count on
   the FP64 plan) and the oracle;
-* its result is the same alone and admitted into a mix whose slots sit at other iterations, and next to a
-  slot whose limit does not fit the basis (that slot runs CGS GMRES(basis) in the same engine).
+* its result is the same alone and admitted into a mix whose slots sit at other iterations;
+* a slot whose limit does not fit the basis restarts when the basis is full, every floor(basis / 8) * 8
+  iterations, and matches GMRES with that restart length.
 """
 import numpy as np
 import pytest
@@ -78,8 +79,8 @@ def test_block_engine_alone_matches_block_solve_and_oracle(precision):
 
 @pytest.mark.parametrize("precision", ["float64", "float32-math64"])
 def test_block_engine_same_alone_and_in_mix_with_cgs_slot(precision):
-    """A alone, then A admitted while B (block) runs, next to C whose limit (120 iterations) does not fit
-    the basis with a block (C runs CGS GMRES(112) in the same engine); fewer slots than right-hand sides."""
+    """A alone, then A admitted while B runs, next to C whose limit (120 iterations) does not fit the basis
+    (C restarts after 112 iterations, as GMRES(112)); fewer slots than right-hand sides."""
     a_alone = _request(0, 21, 2)
     eng = SV.Engine(_solver(precision), slots=3, basis=BASIS, wavelength=WL, permittivity_bg=EPS_BG, ortho="block")
     try:
@@ -109,3 +110,19 @@ def test_block_engine_same_alone_and_in_mix_with_cgs_slot(precision):
     if precision == "float64":
         assert c.infos[0]["iterations"] == info[0]["iterations"]
 
+
+def test_block_engine_restarts_like_gmres_restart():
+    """basis 24 < iteration limit: block cycles of 24 iterations (8 CGS steps and two blocks), as GMRES(24)."""
+    req = _request(5, 31, 2)
+    eng = SV.Engine(_solver("float64"), slots=2, basis=24, wavelength=WL, permittivity_bg=EPS_BG, ortho="block")
+    try:
+        eng.submit(req)
+        eng.drain([req])
+    finally:
+        eng.close()
+    ref, info = _batch_reference(req, "float64", ortho="cgs", restart=24)
+    for b in range(2):
+        assert req.infos[b]["iterations"] == info[b]["iterations"]
+        assert req.infos[b]["iterations"] > 24
+        assert rel(req.E[..., b], ref[b].E) < 1e-10
+        assert rel(req.H[..., b], ref[b].H) < 1e-10
