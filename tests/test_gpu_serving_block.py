@@ -126,3 +126,27 @@ def test_block_engine_restarts_like_gmres_restart():
         assert req.infos[b]["iterations"] > 24
         assert rel(req.E[..., b], ref[b].E) < 1e-10
         assert rel(req.H[..., b], ref[b].H) < 1e-10
+
+
+@pytest.mark.parametrize("grid", [(15, 12, 10), (15, 13, 9)])
+def test_block_engine_on_general_grids(grid):
+    """Odd and non-power-of-two axes (the general passes).  On 15x12x10 (3 x padded voxels a multiple of 4) the
+    slots run block GMRES; on 15x13x9 they cannot and run CGS in the same block engine.  Either way the engine
+    matches the batched solve of the same method on the FP64 plan."""
+    med = F.phantom_random_beads(grid, 2, (1.5, 3.0), (1.36, 1.60), EPS_BG, 41)
+    cone = F.illumination_cone(grid, RES, WL, EPS_BG, 2, 1.2, 41)
+    req = SV.Request(req_id=7, medium=med, sources=cone[:2], tolerance=1e-6)
+    eng = SV.Engine(_solver("float64", grid), slots=2, basis=BASIS, wavelength=WL, permittivity_bg=EPS_BG,
+                    ortho="block")
+    try:
+        eng.submit(req)
+        eng.drain([req])
+    finally:
+        eng.close()
+    n = int(np.prod(_solver("float64", grid).padded_size()))
+    ortho = "block" if (3 * n) % 4 == 0 else "cgs"
+    ref, info = _batch_reference(req, "float64", ortho=ortho)
+    for b in range(2):
+        assert req.infos[b]["iterations"] == info[b]["iterations"]
+        assert rel(req.E[..., b], ref[b].E) < 1e-10
+        assert rel(req.H[..., b], ref[b].H) < 1e-10
