@@ -383,7 +383,8 @@ def run(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_med * 1000.0, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+                "vs_baseline": None, "dtype": "c128" if args.precision == "float32-math64" else "c64",
+                "data": "synthetic",
                 "config": {"workload": "batching: 128x128x64 (padded 128^3), 12 seeded beads, "
                                        f"{nrhs} RHS per GPU ({nrhs // 2} NA-1.2 angles x 2 pol), "
                                        f"GMRES-{opts.maxiters}",
