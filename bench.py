@@ -528,6 +528,40 @@ def large_check(args):
             "residual_ratio": r32 / r64 if r64 else None}
 
 
+def run_two_beam_example(args):
+    """The reference's examples/two_beam_interference.jl homogeneous case: 201x201x191 at 50 nm (odd axes, the
+    general passes), periodic x/y, 300 nm Tanh absorbing z, water, two coherent x-polarised 532 nm waves at the
+    +-3rd order, BiCGStab, tolerance 1e-6.  Each precision's solve is timed from host arrays to host fields
+    (wall clock, after one untimed solve for the plan and tables), with the example's fringe contrast."""
+    import fmcuda as F
+    grid, res = (201, 201, 191), (50e-9,) * 3
+    bc_z = F.AbsorbingBoundaryCondition(thickness=300e-9, attenuation_thickness=300e-9, sharpness=1.0,
+                                        profile=F.TanhProfile)
+    bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
+    eps_bg, wl = 1.333 ** 2, 532e-9
+    ky = 2 * math.pi * 3 / (grid[1] * res[1])
+    a = math.asin(ky / (2 * math.pi * math.sqrt(eps_bg) / wl))
+    srcs = [F.PlaneWaveSource(wavelength=wl, polarization=[1.0, 0.0, 0.0], k_vector=[0.0, sg * math.sin(a),
+                                                                                   math.cos(a)]) for sg in (1, -1)]
+    med = F.Medium(np.full(grid, eps_bg, dtype=np.complex128), eps_bg)
+    out = {"grid": list(grid), "solver": "bicgstab", "tolerance": 1e-6}
+    for prec in ("float64", args.precision):
+        sv = F.ConvergentBornSolver(resolution=res, grid_size=grid, boundary_conditions=bcs, tolerance=1e-6,
+                                    precision=prec, linear_solver=F.KrylovJL_BICGSTAB())
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            F.solve(sv, srcs, med)
+            t0 = time.perf_counter()
+            f = F.solve(sv, srcs, med)
+            dt = time.perf_counter() - t0
+        it = np.sum(np.abs(f.E) ** 2, axis=3)[grid[0] // 2, :, grid[2] // 2]
+        out[prec] = {"seconds_per_solve": dt, "iterations": sv.iteration_count,
+                     "padded": list(sv.padded_size()),
+                     "contrast": float((it.max() - it.min()) / (it.max() + it.min()))}
+        sv.release()
+    return out
+
+
 def run_operator_case(args):
     """Small case for profilers: `reps` applications of the CBS operator on `nrhs` seeded random fields
     on the bench grid (no solve)."""
@@ -573,14 +607,19 @@ def main():
     ap.add_argument("--serving-requests", type=int, default=8, help="requests in the serving sample (0: skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0)
     ap.add_argument("--serving-budget-gb", type=float, default=150.0)
-    ap.add_argument("--serving-basis", type=int, default=112, help="Krylov basis per slot (block slots need "
-                    "maxiters + 8 <= basis)")
+    ap.add_argument("--serving-basis", type=int, default=112, help="Krylov basis per slot (block slots run full "
+                    "GMRES when maxiters + 8 <= basis, else restart when the basis is full)")
     ap.add_argument("--serving-ortho", default="block", choices=["cgs", "cgs2", "block"])
     ap.add_argument("--serving-only", action="store_true", help="run the serving sample alone and print it")
     ap.add_argument("--large-only", action="store_true", help="run the large single configuration and print it")
     ap.add_argument("--large-check", type=int, default=1, help="with the large configuration: FP32 vs FP64 check at 128x128x256")
     ap.add_argument("--large", type=int, default=1, help="1: also run the large single configuration (N = 1 only)")
+    ap.add_argument("--example-two-beam", action="store_true",
+                    help="time the reference's examples/two_beam_interference.jl solve (201x201x191, BiCGStab)")
     args = ap.parse_args()
+    if args.example_two_beam:
+        print(json.dumps({"two_beam_example": run_two_beam_example(args)}))
+        return 0
     if args.operator_case:
         return run_operator_case(args)
     if args.serving_only:
