@@ -562,6 +562,34 @@ def run_two_beam_example(args):
     return out
 
 
+def run_basic_example(args):
+    """The reference's examples/basic_scattering.jl: 128x128x64 at 50 nm, periodic x/y, 3 um Tanh absorbing z
+    (padded z 124, the general passes), a SiO2 bead (n = 1.46, radius 10 px) in water, an x-polarised 532 nm
+    plane wave along +z, GMRES, tolerance 1e-2.  Each precision's solve is timed from host arrays to host fields
+    (wall clock, after one untimed solve for the plan and tables), the bead painted on the device."""
+    import fmcuda as F
+    grid, res, eps_bg = (128, 128, 64), (50e-9,) * 3, 1.333 ** 2
+    bc_z = F.AbsorbingBoundaryCondition(thickness=3e-6, attenuation_thickness=3e-6, sharpness=1.0,
+                                        profile=F.TanhProfile)
+    bcs = (F.PeriodicBoundaryCondition(), F.PeriodicBoundaryCondition(), bc_z)
+    src = F.PlaneWaveSource(wavelength=532e-9, polarization=[1.0, 0.0, 0.0], k_vector=[0.0, 0.0, 1.0])
+    med = F.phantom_bead(grid, [1.46 ** 2], 10.0, permittivity_bg=eps_bg, on_device=True)
+    out = {"grid": list(grid), "solver": "gmres", "tolerance": 1e-2}
+    for prec in ("float64", args.precision):
+        sv = F.ConvergentBornSolver(resolution=res, grid_size=grid, boundary_conditions=bcs, tolerance=1e-2,
+                                    precision=prec, linear_solver=F.KrylovJL_GMRES())
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            F.solve(sv, src, med)
+            t0 = time.perf_counter()
+            f = F.solve(sv, src, med)
+            dt = time.perf_counter() - t0
+        out[prec] = {"seconds_per_solve": dt, "iterations": sv.iteration_count, "padded": list(sv.padded_size()),
+                     "max_abs_E": float(np.abs(f.E).max())}
+        sv.release()
+    return out
+
+
 def run_operator_case(args):
     """Small case for profilers: `reps` applications of the CBS operator on `nrhs` seeded random fields
     on the bench grid (no solve)."""
@@ -616,7 +644,12 @@ def main():
     ap.add_argument("--large", type=int, default=1, help="1: also run the large single configuration (N = 1 only)")
     ap.add_argument("--example-two-beam", action="store_true",
                     help="time the reference's examples/two_beam_interference.jl solve (201x201x191, BiCGStab)")
+    ap.add_argument("--example-basic", action="store_true",
+                    help="time the reference's examples/basic_scattering.jl solve (128x128x64 bead, GMRES)")
     args = ap.parse_args()
+    if args.example_basic:
+        print(json.dumps({"basic_scattering_example": run_basic_example(args)}))
+        return 0
     if args.example_two_beam:
         print(json.dumps({"two_beam_example": run_two_beam_example(args)}))
         return 0
