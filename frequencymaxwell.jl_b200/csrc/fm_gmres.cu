@@ -431,8 +431,8 @@ static cudaError_t launch_blockdot(fm_plan* P, int nb, int K, const void* U, con
 
 // Z = Y - X E and the Gram matrix of Z.  TZ: type of Z (the basis type, or the block-vector type when the block
 // is stored orthonormalised afterwards and Z overwrites Y in place).  The Gram goes to red_out: the upper triangle
-// tri(t,u) for S <= 8 (k_blockgram), the full S x S matrix <Z_t, Z_u> at t*S + u for S > 8 (the block dot of Z
-// against itself on the tensor cores).
+// tri(t,u) for S <= 8 (accumulated by the update kernel itself from the values it stores), the full S x S matrix
+// <Z_t, Z_u> at t*S + u for S > 8 (the block dot of Z against itself on the tensor cores, a second pass).
 template <typename R, typename YR, int S, typename TZ>
 static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, const void* Y, void* Z, const int* act,
                                       int nact, const int* Kb) {
@@ -440,15 +440,23 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
   using TY = cplx<YR>;
   constexpr int NG = S * (S + 1) / 2;
   constexpr int TILE = S <= 8 ? 32 : 16;  // elements per warp tile of k_blockupdate_mma
-  auto kern = k_blockupdate_mma<R, TY, S, TZ>;
+  auto kern = k_blockupdate_mma<R, TY, S, TZ, (S <= 8)>;
   int bps = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, KV_THREADS, 0) != cudaSuccess || bps < 1) bps = 1;
   const long long maxb = (P->M + TILE * KV_WARPS - 1) / (TILE * KV_WARPS);
   const int nblk = (int)std::max(1LL, std::min<long long>(maxb, (long long)P->sms * bps / nb));
+  cudaError_t e = cudaSuccess;
+  if constexpr (S <= 8) {
+    e = P->red_part.ensure((size_t)nb * nblk * NG * sizeof(double2));
+    if (e == cudaSuccess) e = P->red_out.ensure((size_t)nb * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
+    if (e != cudaSuccess) return e;
+  }
   FM_TRACK(P, KC_UPD, ((double)K * sizeof(T) + (double)S * (sizeof(TY) + sizeof(TZ))) * nact * P->M,
            (kern<<<dim3(nblk, nb), KV_THREADS, 0, P->st>>>(P->M, nb, K, (const T*)U, (const TY*)Y, (TZ*)Z,
-                                                            (const double2*)P->coef.p, act, Kb)));
-  cudaError_t e = cudaGetLastError();
+                                                            (const double2*)P->coef.p, act, Kb,
+                                                            (double2*)P->red_part.p, (double2*)P->red_out.p,
+                                                            (unsigned*)P->red_cnt.p)));
+  e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   if constexpr (S > 8) {
     using ZR = typename RealOf<TZ>::R;
@@ -465,16 +473,8 @@ static cudaError_t launch_blockupdate(fm_plan* P, int nb, int K, const void* U, 
                                                              (double2*)P->red_part.p, (double2*)P->red_out.p,
                                                              (unsigned*)P->red_cnt.p, act, nullptr)));
     return cudaGetLastError();
-  } else {
-    const int nblk_g = kv_blocks(P, k_blockgram<R, S, TZ>, nb);
-    e = P->red_part.ensure((size_t)nb * nblk_g * (std::max)(NG, KV_KMAX + 2) * sizeof(double2));
-    if (e != cudaSuccess) return e;
-    FM_TRACK(P, KC_MGS, (double)S * sizeof(TZ) * nact * P->M,
-             (k_blockgram<R, S, TZ><<<dim3(nblk_g, nb), KV_THREADS, 0, P->st>>>(
-                 P->M, nb, (const TZ*)Z, (double2*)P->red_part.p, (double2*)P->red_out.p, (unsigned*)P->red_cnt.p,
-                 act)));
-    return cudaGetLastError();
   }
+  return cudaSuccess;
 }
 
 // V (basis slots) = Z Rb^{-1} for the orthonormalised block storage; coefficients in P->coef

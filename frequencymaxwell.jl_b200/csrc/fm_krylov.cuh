@@ -508,22 +508,40 @@ __device__ __forceinline__ void load_run(const C* p, C (&v)[QR]) {
 // gid: elements QR gid .. QR gid + QR - 1 of the tile) and runs over the basis 4 vectors at a time.  B tiles as in
 // k_blockdot_mma; x c:  Re = P[t] - Q[4+t], Im = P[4+t] + Q[t]  (one tile) or, for t = 8h + c,
 // Re = P[h][c] - Q[NTH + h][c],  Im = P[NTH + h][c] + Q[h][c].  Optional per-RHS basis sizes Kb[b] <= K.
-template <typename R, typename TY, int S, typename TZ = cplx<R>>
+//
+// GRAM (S <= 8): the Gram matrix of the stored Z is accumulated on the way out, so that no second pass reads Z:
+// out[b][tri(t,u)] = <Z_t, Z_u> for t <= u, tri(t,u) = t*S - t*(t-1)/2 + (u-t) (FP64, deterministic).  Each warp
+// passes its tile through shared memory in two halves of 16 elements (lane (gid, tig) of the update holds elements
+// 4 gid + q, columns 2 tig + i), and four k-steps of m8n8k4 MMAs per half take A = Z^H, B = Z with lane (gid, tig)
+// holding Z[element tig of the k-step][column gid] for both operands.  Rows r of a half sit at r*8 + (t ^ gram_swz(r)),
+// which keeps both the column-pair stores and the fragment loads free of bank conflicts.
+__device__ __forceinline__ int gram_swz(int r) { return (2 * (r & 3)) ^ ((r >> 1) & 1); }
+
+template <typename R, typename TY, int S, typename TZ = cplx<R>, bool GRAM = false>
 __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, int B, int K, const cplx<R>* U,
                                                                 const TY* Y, TZ* Z,
                                                                 const double2* __restrict__ coef,
                                                                 const int* __restrict__ active,
-                                                                const int* __restrict__ Kb = nullptr) {
+                                                                const int* __restrict__ Kb = nullptr,
+                                                                double2* __restrict__ gpart = nullptr,
+                                                                double2* __restrict__ gout = nullptr,
+                                                                unsigned* __restrict__ gcounter = nullptr) {
   static_assert(S >= 1 && S <= 16, "block update on tensor cores takes 1..16 block vectors");
+  static_assert(!GRAM || S <= 8, "the fused Gram takes at most 8 block vectors");
   using T = cplx<R>;
   constexpr int NTH = S <= 4 ? 1 : (S + 7) / 8;
   constexpr int NT = S <= 4 ? 1 : 2 * NTH;
   constexpr int QR = S <= 8 ? 4 : 2;  // elements per lane (A rows of QR MMAs)
   constexpr int TILE = 8 * QR;        // elements per warp tile
   __shared__ double Bs[KV_KMAX][8 * NT];
+  __shared__ double2 zs[GRAM ? KV_WARPS * 128 : 1];       // one half tile (16 elements x 8 columns) per warp
+  __shared__ double gacc[GRAM ? KV_WARPS * 4 * 32 : 1];  // per warp and lane: Re G[gid][2 tig + i], Im G[..]
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   if (Kb) K = Kb[b];
+  if constexpr (GRAM) {
+    for (int i = threadIdx.x; i < KV_WARPS * 4 * 32; i += blockDim.x) gacc[i] = 0.0;
+  }
   for (int i = threadIdx.x; i < KV_KMAX * 8 * NT; i += blockDim.x) {
     const int k = i / (8 * NT), col = i - k * (8 * NT);
     int t;
@@ -600,9 +618,12 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
       }
     }
     // lane (gid, tig) holds C rows gid (element ea + q) and columns 2 tig, 2 tig + 1 of each tile
+    double g[4] = {0.0, 0.0, 0.0, 0.0};  // this tile's Gram fragment (GRAM)
+    double2* zw = zs + (GRAM ? w * 128 : 0);
 #pragma unroll
     for (int q = 0; q < QR; ++q) {
       const long long e = ea + q;
+      double2 zq[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};  // stored values of columns 2 tig + i
       if constexpr (NT == 1) {
         const double pp0 = __shfl_xor_sync(0xffffffffu, P[q][0][0], 2), pp1 = __shfl_xor_sync(0xffffffffu, P[q][0][1], 2);
         const double qp0 = __shfl_xor_sync(0xffffffffu, Q[q][0][0], 2), qp1 = __shfl_xor_sync(0xffffffffu, Q[q][0][1], 2);
@@ -610,11 +631,15 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
           const int t0 = 2 * tig;
           if (t0 < S) {
             const double2 y = to_d(yb[t0 * us + e]);
-            zb[t0 * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][0] - qp0), y.y - (pp0 + Q[q][0][0])));
+            const TZ z = from_d<TZ>(make_double2(y.x - (P[q][0][0] - qp0), y.y - (pp0 + Q[q][0][0])));
+            zb[t0 * us + e] = z;
+            zq[0] = to_d(z);
           }
           if (t0 + 1 < S) {
             const double2 y = to_d(yb[(t0 + 1) * us + e]);
-            zb[(t0 + 1) * us + e] = from_d<TZ>(make_double2(y.x - (P[q][0][1] - qp1), y.y - (pp1 + Q[q][0][1])));
+            const TZ z = from_d<TZ>(make_double2(y.x - (P[q][0][1] - qp1), y.y - (pp1 + Q[q][0][1])));
+            zb[(t0 + 1) * us + e] = z;
+            zq[1] = to_d(z);
           }
         }
       } else if (ein) {
@@ -625,62 +650,58 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
             const int t = 8 * th + 2 * tig + i;
             if (t < S) {
               const double2 y = to_d(yb[t * us + e]);
-              zb[t * us + e] = from_d<TZ>(make_double2(y.x - (P[q][th][i] - Q[q][NTH + th][i]),
-                                                      y.y - (P[q][NTH + th][i] + Q[q][th][i])));
+              const TZ z = from_d<TZ>(make_double2(y.x - (P[q][th][i] - Q[q][NTH + th][i]),
+                                                   y.y - (P[q][NTH + th][i] + Q[q][th][i])));
+              zb[t * us + e] = z;
+              if (th == 0) zq[i] = to_d(z);
             }
           }
       }
-    }
-  }
-}
-
-// Gram matrix of S stored vectors Z_t = Z[(t*B + b)*M]:  out[b][tri(t,u)] = <Z_t, Z_u>, t <= u,
-// tri(t,u) = t*S - t*(t-1)/2 + (u-t)   (FP64 accumulation, deterministic).
-template <typename R, int S, typename TZ = cplx<R>>
-__global__ void __launch_bounds__(KV_THREADS) k_blockgram(long long M, int B, const TZ* __restrict__ Z,
-                                                          double2* __restrict__ part, double2* __restrict__ out,
-                                                          unsigned* __restrict__ counter,
-                                                          const int* __restrict__ active) {
-  constexpr int NG = S * (S + 1) / 2;
-  __shared__ double2 red[KV_WARPS][NG];
-  const int b = blockIdx.y, nblk = gridDim.x;
-  if (active && !active[b]) return;
-  double2 gram[NG];
+      if constexpr (GRAM) {
+        const int r = 2 * gid + (q & 1);  // row of element 4 gid + q in its half
 #pragma unroll
-  for (int i = 0; i < NG; ++i) gram[i] = make_double2(0.0, 0.0);
-  const TZ* zb = Z + (size_t)b * M;
-  const size_t us = (size_t)B * M;
-  const long long per = (M + nblk - 1) / nblk;
-  const long long lo = (long long)blockIdx.x * per, hi = min(M, lo + per);
-  for (long long e = lo + threadIdx.x; e < hi; e += blockDim.x) {
-    double2 st[S];
+        for (int i = 0; i < 2; ++i) zw[r * 8 + ((2 * tig + i) ^ gram_swz(r))] = zq[i];
+        if (q & 1) {
+          __syncwarp();
 #pragma unroll
-    for (int t = 0; t < S; ++t) st[t] = to_d(zb[t * us + e]);
-    int gi = 0;
-#pragma unroll
-    for (int t = 0; t < S; ++t)
-#pragma unroll
-      for (int u = t; u < S; ++u, ++gi) {
-        gram[gi].x = fma(st[t].x, st[u].x, fma(st[t].y, st[u].y, gram[gi].x));
-        gram[gi].y = fma(st[t].x, st[u].y, fma(-st[t].y, st[u].x, gram[gi].y));
+          for (int j = 0; j < 4; ++j) {
+            const int rr = 4 * j + tig;
+            const double2 v = zw[rr * 8 + (gid ^ gram_swz(rr))];
+            mma_f64(g[0], g[1], v.x, v.x);   // Re += zr_t zr_u
+            mma_f64(g[0], g[1], v.y, v.y);   //    + zi_t zi_u
+            mma_f64(g[2], g[3], v.x, v.y);   // Im += zr_t zi_u
+            mma_f64(g[2], g[3], -v.y, v.x);  //    - zi_t zr_u
+          }
+          __syncwarp();
+        }
       }
-  }
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < NG; ++i) {
-    const double2 v = warp_sum(gram[i]);
-    if (lane == 0) red[wi][i] = v;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < NG; i += blockDim.x) {
-    double2 sum = make_double2(0.0, 0.0);
-    for (int q = 0; q < KV_WARPS; ++q) {
-      sum.x += red[q][i].x;
-      sum.y += red[q][i].y;
     }
-    part[((size_t)b * nblk + blockIdx.x) * NG + i] = sum;
+    if constexpr (GRAM) {
+      double* ga = gacc + w * 128 + lane;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ga[32 * c] += g[c];
+    }
   }
-  finish_reduce(part, out, counter, NG, nblk, b);
+  if constexpr (GRAM) {
+    // CTA sum over the warps, then the grid-wide sum per RHS (deterministic order)
+    constexpr int NG = S * (S + 1) / 2;
+    __syncthreads();
+    for (int o = threadIdx.x; o < NG; o += blockDim.x) {
+      int t = 0, rem = o;
+      while (rem >= S - t) {
+        rem -= S - t;
+        ++t;
+      }
+      const int u = t + rem, ln = 4 * t + (u >> 1), i = u & 1;
+      double2 s = make_double2(0.0, 0.0);
+      for (int q = 0; q < KV_WARPS; ++q) {
+        s.x += gacc[q * 128 + 32 * i + ln];
+        s.y += gacc[q * 128 + 32 * (2 + i) + ln];
+      }
+      gpart[((size_t)b * gridDim.x + blockIdx.x) * NG + o] = s;
+    }
+    finish_reduce(gpart, gout, gcounter, NG, gridDim.x, b);
+  }
 }
 
 // Orthonormal block from the projected block vectors:  V_t[b] = sum_{u <= t} Z_u[b] c[b][u*S + t]
