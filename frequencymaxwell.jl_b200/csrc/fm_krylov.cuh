@@ -533,7 +533,10 @@ __global__ void __launch_bounds__(KV_THREADS, 2) k_blockupdate_mma(long long M, 
   constexpr int NT = S <= 4 ? 1 : 2 * NTH;
   constexpr int QR = S <= 8 ? 4 : 2;  // elements per lane (A rows of QR MMAs)
   constexpr int TILE = 8 * QR;        // elements per warp tile
-  __shared__ double Bs[KV_KMAX][8 * NT];
+  // coefficient rows padded to 4 (mod 16) doubles: the B-fragment loads (row kk + tig, column 8n + gid) then put
+  // the four rows of a k-step 8 banks apart, two lanes per bank pair, the minimum for 256 bytes
+  constexpr int BROW = (8 * NT + 15) / 16 * 16 + 4;
+  __shared__ double Bs[KV_KMAX][BROW];
   __shared__ double2 zs[GRAM ? KV_WARPS * 128 : 1];       // one half tile (16 elements x 8 columns) per warp
   __shared__ double gacc[GRAM ? KV_WARPS * 4 * 32 : 1];  // per warp and lane: Re G[gid][2 tig + i], Im G[..]
   const int b = blockIdx.y;
