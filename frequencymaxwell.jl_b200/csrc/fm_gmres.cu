@@ -631,7 +631,9 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
                    P->M, nb, k0, nc, U, (const double2*)P->coef.p, 16, Yb, act)));
       FM_CK(cudaGetLastError());
     }
-    // Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}, t = 1..S
+    // Y_t = M^{-1}A Y_{t-1} - theta_t Y_{t-1}, t = 1..S; on the fused passes the x pass of application t+1 runs
+    // inside the last pass of application t (GREEN_CHAIN_*), so Y_t and V are not read back for it
+    const bool chainable = green_chain_ok(P, &rcY);
     std::vector<double2> th(nb);
     for (int t = 1; t <= S; ++t) {
       for (int b = 0; b < nb; ++b) th[b] = make_double2(St[b].theta[t - 1].real(), St[b].theta[t - 1].imag());
@@ -641,7 +643,8 @@ static fm_status gmres_block(fm_plan* P, int nb, const fm_solve_opts& o, std::ve
       TY* Yin = Yb + (size_t)(t - 1) * nb * fe;
       TY* Yout = Yb + (size_t)t * nb * fe;
       // (the shift array is rewritten for the next vector in stream order, after this pass has read it)
-      FM_TRY(green_op<YR>(P, nb, Yin, PRO_V, nullptr, EPI_PREC_OP, Yin, nullptr, eps, Yout, act, nact, &rcY));
+      const int chain = !chainable ? 0 : (t > 1 ? GREEN_CHAIN_HAVE_XF : 0) | (t < S ? GREEN_CHAIN_NEXT_XF : 0);
+      FM_TRY(green_op<YR>(P, nb, Yin, PRO_V, nullptr, EPI_PREC_OP, Yin, nullptr, eps, Yout, act, nact, &rcY, chain));
     }
     // D = X^H Y_{1..S}
     FM_CK((block_kernels<R, YR>(P, 0, S, nb, K, U, Yb + (size_t)nb * fe, nullptr, act, nact)));

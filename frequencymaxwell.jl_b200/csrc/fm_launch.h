@@ -27,6 +27,11 @@ template <typename S, typename R>
 cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, const void* xv, const void* bv,
                       const double* rhs_scale, const EpiParams& ep, const void* twx, const void* rampx, void* out,
                       const int* active, cudaStream_t st, VecTab vt = VecTab{});
+// XI with EPI_PREC_OP (no x ramp, contiguous batches) and the next application's XF (PRO_V) of its result:
+// out = the operator result, out2 = the x-transformed V .* out
+template <typename S, typename R>
+cudaError_t launch_xi_xf(const Dims& d, const void* in, const void* V, const void* xv, const EpiParams& ep,
+                         const void* twx, void* out, void* out2, const int* active, cudaStream_t st);
 
 // TMA-staged y and z passes (fm_passes_tma.cuh).  They return cudaErrorNotSupported when the
 // shape has no TMA variant (the caller then uses the register-only passes).  `err` receives a

@@ -121,8 +121,14 @@ static fm_status gen_green_op(fm_plan* P, int nb, const void* in, int pro, const
 
 template <typename R>
 fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
-                   const void* bv, const EpiParams& ep_in, void* out, const int* act, int nact, const RhsCtx* rc) {
+                   const void* bv, const EpiParams& ep_in, void* out, const int* act, int nact, const RhsCtx* rc,
+                   int chain) {
   using T = cplx<R>;
+  if (chain) {
+    if (!green_chain_ok(P, rc) || ((chain & GREEN_CHAIN_HAVE_XF) && pro != PRO_V) ||
+        ((chain & GREEN_CHAIN_NEXT_XF) && (epi != EPI_PREC_OP || rs || xv != in)))
+      return fail(FM_ERR_INVALID, "operator chaining needs the fused passes, PRO_V and EPI_PREC_OP on the input");
+  }
   if (P->generic) return gen_green_op<R>(P, nb, in, pro, rs, epi, xv, bv, ep_in, out, act, nact, rc);
   if (nact < 0) nact = nb;
   EpiParams ep = ep_in;
@@ -156,9 +162,11 @@ fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs
     gp.shift[2] = P->zonly ? P->shift[2] : 0.0;
     gp.scale_re = 1.0 / ((double)P->n * (P->zonly ? 2.0 : 1.0));
     cudaError_t e;
-    FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
-             e = pass_xf<R>(P, d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act, vt));
-    FM_CK(e);
+    if (!(chain & GREEN_CHAIN_HAVE_XF)) {
+      FM_TRACK(P, KC_XF, 2 * fbA + (pro != PRO_COPY ? vb : 0.0),
+               e = pass_xf<R>(P, d, pro, in, V, rs, P->twx.p, nullptr, P->t1.p, act, vt));
+      FM_CK(e);
+    }
     FM_TRACK(P, KC_YF, 2 * fbA, e = pass_y<R>(P, d, -1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
     FM_CK(e);
     FM_TRACK(P, KC_ZG, 2 * fbA,
@@ -167,7 +175,10 @@ fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs
     FM_CK(e);
     FM_TRACK(P, KC_YI, 2 * fbA, e = pass_y<R>(P, d, +1, P->t1.p, P->twy.p, nullptr, P->t2.p, act));
     FM_CK(e);
-    FM_TRACK(P, KC_XI, xib, e = pass_xi<R>(P, d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act, vt));
+    if (chain & GREEN_CHAIN_NEXT_XF)
+      FM_TRACK(P, KC_XI, xib + fbA, e = pass_xi_xf<R>(P, d, P->t2.p, V, xv, ep, P->twx.p, out, P->t1.p, act));
+    else
+      FM_TRACK(P, KC_XI, xib, e = pass_xi<R>(P, d, epi, P->t2.p, V, xv, bv, rs, ep, P->twx.p, nullptr, out, act, vt));
     FM_CK(e);
     return FM_OK;
   }
@@ -288,8 +299,8 @@ fm_status curl_batch(fm_plan* P, int nb, const void* in, void* out, const int* a
 }
 
 template fm_status green_op<float>(fm_plan*, int, const void*, int, const double*, int, const void*, const void*,
-                                   const EpiParams&, void*, const int*, int, const RhsCtx*);
+                                   const EpiParams&, void*, const int*, int, const RhsCtx*, int);
 template fm_status green_op<double>(fm_plan*, int, const void*, int, const double*, int, const void*, const void*,
-                                    const EpiParams&, void*, const int*, int, const RhsCtx*);
+                                    const EpiParams&, void*, const int*, int, const RhsCtx*, int);
 template fm_status curl_batch<float>(fm_plan*, int, const void*, void*, const int*);
 template fm_status curl_batch<double>(fm_plan*, int, const void*, void*, const int*);

@@ -12,6 +12,8 @@ template cudaError_t launch_xi<float, float>(const Dims&, int, const void*, cons
                                       const double*, const EpiParams&, const void*, const void*, void*, const int*,
                                       cudaStream_t, VecTab);
 template int pencils_per_warp<float>(int);
+template cudaError_t launch_xi_xf<float, float>(const Dims&, const void*, const void*, const void*, const EpiParams&,
+                                         const void*, void*, void*, const int*, cudaStream_t);
 template cudaError_t launch_y_tma<float, float>(const Dims&, int, const void*, const void*, const void*, void*,
                                           const int*, int*, int, cudaStream_t);
 template cudaError_t launch_zg_tma<float, float>(const Dims&, int, const void*, const GreenParams&, const void*,

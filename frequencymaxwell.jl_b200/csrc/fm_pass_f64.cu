@@ -12,6 +12,8 @@ template cudaError_t launch_xi<double, double>(const Dims&, int, const void*, co
                                       const double*, const EpiParams&, const void*, const void*, void*, const int*,
                                       cudaStream_t, VecTab);
 template int pencils_per_warp<double>(int);
+template cudaError_t launch_xi_xf<double, double>(const Dims&, const void*, const void*, const void*, const EpiParams&,
+                                         const void*, void*, void*, const int*, cudaStream_t);
 template cudaError_t launch_y_tma<double, double>(const Dims&, int, const void*, const void*, const void*, void*,
                                           const int*, int*, int, cudaStream_t);
 template cudaError_t launch_zg_tma<double, double>(const Dims&, int, const void*, const GreenParams&, const void*,

@@ -52,6 +52,24 @@ static cudaError_t xi_L(const Dims& d, const void* in, const void* V, const void
   return cudaGetLastError();
 }
 
+template <typename S, typename R, int L>
+static cudaError_t xi_xf_L(const Dims& d, const void* in, const void* V, const void* xv, const EpiParams& ep,
+                           const void* tw, void* out, void* out2, const int* act, cudaStream_t st) {
+  using T = cplx<R>;
+  using TS = cplx<S>;
+  using P_ = Plan<L, R>;
+  constexpr int PW = 32 / P_::TP;
+  const int W = row_threads(d) / 32;
+  const long long rows = (long long)d.ny * d.nz * d.nb;
+  const long long warps = rows / PW;
+  const unsigned blocks = (unsigned)((warps + W - 1) / W);
+  const size_t smem = (size_t)(2 * L + W * PW * PencilStride<L, T, P_::TP, true>::v) * sizeof(T);
+  allow_smem(k_xi_xf<S, R, L>, smem);
+  k_xi_xf<S, R, L><<<blocks, W * 32, smem, st>>>(d, (const TS*)in, (const TS*)V, (const TS*)xv, ep, (const T*)tw,
+                                                 (TS*)out, (TS*)out2, act);
+  return cudaGetLastError();
+}
+
 template <typename S, typename R, int L, int DIR>
 static cudaError_t y_L(const Dims& d, const void* in, const void* tw, const void* ramp, void* out, const int* act,
                        cudaStream_t st) {
@@ -154,6 +172,14 @@ cudaError_t launch_xi(const Dims& d, int epi, const void* in, const void* V, con
 #undef XI1
 #undef XI2
 #undef XI3
+}
+
+template <typename S, typename R>
+cudaError_t launch_xi_xf(const Dims& d, const void* in, const void* V, const void* xv, const EpiParams& ep,
+                         const void* tw, void* out, void* out2, const int* act, cudaStream_t st) {
+#define XX(LL) xi_xf_L<S, R, LL>(d, in, V, xv, ep, tw, out, out2, act, st)
+  FM_SWITCH_L(d.nx, XX, XX)
+#undef XX
 }
 
 template <typename S, typename R>

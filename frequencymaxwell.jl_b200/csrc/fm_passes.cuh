@@ -494,4 +494,69 @@ __global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 3 : 1) k_xi(Dims 
   }
 }
 
+// XI with EPI_PREC_OP followed, on the same rows, by the XF pass (PRO_V) of the next operator application:
+//   out  = (i/eps) V (x - g) - theta x          (this application's result, as k_xi stores it)
+//   out2 = FFT_x(V .* out)                      (what k_xf would write from the stored out)
+// Each row's result is still in registers in the R0 layout that the forward transform takes, so the next
+// application's x pass neither reads `out` nor V again.  The forward input is the stored (storage-typed) value,
+// so out2 equals k_xf's output bit for bit.  Contiguous batches and no x ramp (the z-only and periodic plans).
+template <typename S, typename R, int L>
+__global__ void __launch_bounds__(256, (L <= 128 && L != 96) ? 3 : 1) k_xi_xf(Dims d, const cplx<S>* __restrict__ in,
+                                                                          const cplx<S>* __restrict__ V,
+                                                                          const cplx<S>* __restrict__ xv,
+                                                                          EpiParams ep,
+                                                                          const cplx<R>* __restrict__ twx,
+                                                                          cplx<S>* __restrict__ out,
+                                                                          cplx<S>* __restrict__ out2,
+                                                                          const int* __restrict__ active) {
+  using T = cplx<R>;
+  using TS = cplx<S>;
+  using P_ = Plan<L, R>;
+  constexpr int E = P_::E, TP = P_::TP, PW = 32 / TP;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* twf = reinterpret_cast<T*>(smraw);  // forward-order stage twiddles
+  T* twr = twf + L;                      // reversed-order stage twiddles
+  T* ex = twr + L;
+  load_table(twf, twx, 2 * L);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wic = threadIdx.x >> 5;
+  const int p = lane / TP, t = lane % TP;
+  const long long rows = (long long)d.ny * d.nz * d.nb;
+  const long long row = ((long long)blockIdx.x * (blockDim.x >> 5) + wic) * PW + p;
+  if (row >= rows) return;  // whole pencils exit together (rows is a multiple of PW)
+  const int b = (int)(row / ((long long)d.ny * d.nz));
+  if (active && !active[b]) return;
+  const long long yz = row - (long long)b * d.ny * d.nz;
+  T* sm = warp_smem<T, PencilStride<L, T, TP, true>::v>(ex, wic, PW, p);
+  const R ie = ep.inv_eps_b ? (R)ep.inv_eps_b[b] : (R)ep.inv_eps;
+  const cplx<S>* Vrow = V + b * d.vstride + yz * L;
+  const T shf = ep.shift_b ? mk((R)ep.shift_b[b].x, (R)ep.shift_b[b].y) : czero<T>();
+  const T al = mk((R)ep.alpha_re, (R)ep.alpha_im), be = mk((R)ep.beta_re, (R)ep.beta_im);
+  const cplx<S>* xvb = xv + (long long)b * 3 * d.n;
+  cplx<S>* outb = out + (long long)b * 3 * d.n;
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    const long long base = ((long long)(c + 3 * b) * d.ny * d.nz + yz) * L;
+    const long long rbase = ((long long)c * d.ny * d.nz + yz) * L;
+    T v[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) v[e] = cv<T>(in[base + lay_idx<L, E, P_::RL>(t, e)]);
+    fft_rev_plan<+1, P_>(v, sm, twr, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int x = lay_idx<L, E, P_::R0>(t, e);
+      const long long ix = rbase + x;
+      const T r = epi_element<EPI_PREC_OP, S, T, R>(v[e], ix, xvb, nullptr, outb, Vrow + x, ie, R(1), al, be, ep, shf);
+      const TS rs = cv<TS>(r);
+      outb[ix] = rs;
+      v[e] = cmul(cv<T>(rs), cv<T>(Vrow[x]));  // PRO_V of the next application on the stored value
+    }
+    __syncwarp();
+    fft_fwd_plan<-1, P_>(v, sm, twf, t);
+#pragma unroll
+    for (int e = 0; e < E; ++e) out2[base + lay_idx<L, E, P_::RL>(t, e)] = cv<TS>(v[e]);
+    __syncwarp();
+  }
+}
+
 }  // namespace fm

@@ -243,6 +243,14 @@ static cudaError_t pass_xi(const fm_plan* P, const Dims& d, int epi, const void*
   else return P->c64 ? launch_xi<float, double>(d, epi, in, V, xv, bv, rs, ep, tw, ramp, out, act, P->st, vt)
                      : launch_xi<float, float>(d, epi, in, V, xv, bv, rs, ep, tw, ramp, out, act, P->st, vt);
 }
+template <typename S>
+static cudaError_t pass_xi_xf(const fm_plan* P, const Dims& d, const void* in, const void* V, const void* xv,
+                              const EpiParams& ep, const void* tw, void* out, void* out2, const int* act) {
+  if constexpr (std::is_same<S, double>::value)
+    return launch_xi_xf<double, double>(d, in, V, xv, ep, tw, out, out2, act, P->st);
+  else return P->c64 ? launch_xi_xf<float, double>(d, in, V, xv, ep, tw, out, out2, act, P->st)
+                     : launch_xi_xf<float, float>(d, in, V, xv, ep, tw, out, out2, act, P->st);
+}
 
 // ---------------------------------------------------------------------------
 // tables
@@ -356,10 +364,19 @@ struct RhsCtx {
 // ---- operator drivers (fm_ops.cu) ----
 // Green application / CBS operator on device buffers (plan precision): in -> out (nb fields; out may not alias
 // in, t1, t2); pro: PRO_COPY, PRO_V or PRO_V_SCALE applied to `in`; epi: EPI_* applied to g = G_avg(psi).
+// chain (applications in sequence, each on the previous one's output; only where green_chain_ok):
+//   GREEN_CHAIN_HAVE_XF   t1 already holds the x pass of PRO_V on `in` (the previous call left it): skip it
+//   GREEN_CHAIN_NEXT_XF   EPI_PREC_OP whose XI pass also leaves the x pass of PRO_V on `out` in t1
+enum { GREEN_CHAIN_HAVE_XF = 1, GREEN_CHAIN_NEXT_XF = 2 };
 template <typename R>
 fm_status green_op(fm_plan* P, int nb, const void* in, int pro, const double* rs, int epi, const void* xv,
                    const void* bv, const EpiParams& ep_in, void* out, const int* act, int nact = -1,
-                   const RhsCtx* rc = nullptr);
+                   const RhsCtx* rc = nullptr, int chain = 0);
+// the five fused passes (no shift, or z-only shifts in one length-2L z pass), contiguous batches: where green_op
+// can chain applications
+inline bool green_chain_ok(const fm_plan* P, const RhsCtx* rc) {
+  return !P->generic && (!P->avg || P->zonly) && !(rc && (rc->vt.in || rc->vt.out));
+}
 // H = -i lambda/(2 pi 377) curl(E) for nb fields (in -> out, contiguous batches; act masks RHS)
 template <typename R>
 fm_status curl_batch(fm_plan* P, int nb, const void* in, void* out, const int* act);
