@@ -7,6 +7,11 @@ orthogonalisation -- everything else in FP64 -- already moves the iterate by mor
 only the preconditioned operator's outputs.  The FP32-storage forms of the library do both, so on such domains
 they cannot meet 1e-5 whatever their arithmetic; only FP64 storage can.  The same algorithm in FP64 reproduces
 the oracle's iterate to 1e-10.
+
+A defect correction (GMRES restarted every m iterations from the residual recomputed in FP64, the inner basis and
+operator outputs in complex64) does remove the storage error: it agrees with the same scheme run in FP64 to about
+1e-6.  But a restart changes the method: the restarted iterate, in FP64, is several per cent away from the full-GMRES
+iterate at the iteration limit, so no such scheme reproduces the reference's result on a non-converged domain.
 """
 import numpy as np
 import pytest
@@ -63,7 +68,8 @@ def _gmres_rounded(cfg, pot, src, round_basis, round_ops):
     return cfg.crop(x + Ei), cfg.crop(Hs + Hi), j + 1
 
 
-def test_long_domain_iterate_is_sensitive_to_fp32_storage():
+@pytest.fixture(scope="module")
+def long_domain():
     grid = (8, 8, 256)
     t = grid[2] * RES[2]
     cfg = O.SolverConfig(RES, grid, (O.PeriodicBC(), O.PeriodicBC(), O.AbsorbingBC(t, t, 1.0)))
@@ -71,6 +77,11 @@ def test_long_domain_iterate_is_sensitive_to_fp32_storage():
     src = O.PlaneWave(WL, [1, 0, 0], [0, 0, 1])
     ref = O.solve(cfg, src, eps, EPS_BG)
     assert cfg.padded_size[2] == 512 and ref.iterations == 124 and not ref.solved
+    return cfg, src, ref
+
+
+def test_long_domain_iterate_is_sensitive_to_fp32_storage(long_domain):
+    cfg, src, ref = long_domain
     pot = ref.potential
     E, H, it = _gmres_rounded(cfg, pot, src, False, False)
     assert it == ref.iterations
@@ -79,3 +90,43 @@ def test_long_domain_iterate_is_sensitive_to_fp32_storage():
     assert O.rel_l2(E, ref.E) > 1e-5
     E, H, _ = _gmres_rounded(cfg, pot, src, False, True)  # operator outputs in complex64 only
     assert O.rel_l2(E, ref.E) > 1e-5
+
+
+def _defect_corrected(cfg, pot, src, m, total, rounded):
+    """GMRES restarted every m iterations from the FP64 preconditioned residual M^{-1}(b - A x), x kept in FP64;
+    inside a cycle the basis and the operator outputs are rounded to complex64 when `rounded`.  Warm start b,
+    `total` operator applications in all; returns the cropped E."""
+    V, ksq = pot.V, pot.k_square
+    Ei, _ = O.incident_field(src, cfg, EPS_BG)
+    b = O.green_conv(V[..., None] * Ei + (1j * pot.eps_imag) * Ei, cfg, ksq)
+    rop = _round32 if rounded else (lambda a: a)
+    x = b.copy()
+    used = 0
+    while used < total:
+        r = O.cbs_preconditioner(b - O.cbs_operator(x, V, cfg, ksq), V, pot.eps_imag)
+        beta = np.linalg.norm(r)
+        basis = [rop(r / beta)]
+        k = min(m, total - used)
+        H = np.zeros((k + 1, k), complex)
+        g = np.zeros(k + 1, complex)
+        g[0] = beta
+        for j in range(k):
+            w = rop(O.cbs_preconditioner(O.cbs_operator(basis[j], V, cfg, ksq), V, pot.eps_imag))
+            h = np.array([np.vdot(v, w) for v in basis])
+            w = w - sum(hi * v for hi, v in zip(h, basis))
+            H[:j + 1, j] = h
+            H[j + 1, j] = np.linalg.norm(w)
+            basis.append(rop(w / H[j + 1, j]))
+        y = np.linalg.lstsq(H, g, rcond=None)[0]
+        x = x + sum(yi * v for yi, v in zip(y, basis[:k]))
+        used += k
+    return cfg.crop(x + Ei)
+
+
+def test_defect_correction_fixes_precision_not_the_iterate(long_domain):
+    cfg, src, ref = long_domain
+    pot = ref.potential
+    E64 = _defect_corrected(cfg, pot, src, 20, ref.iterations, rounded=False)
+    E32 = _defect_corrected(cfg, pot, src, 20, ref.iterations, rounded=True)
+    assert O.rel_l2(E32, E64) < 1e-5   # measured 1.5e-6: the FP64 defect removes the storage error
+    assert O.rel_l2(E64, ref.E) > 1e-2  # measured 0.19: the restarted method lands elsewhere
